@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark of the VBD hot path on B200: vertex-iterations/s on the 64^3 jittered cube.
+
+Workload (one "step"): one VBDsolver::step of the 274,625-vertex / 1,572,864-tet cube -- predictor,
+50 Gauss-Seidel colour sweeps with the Chebyshev blend (rho 0.9), velocity update -- dt = 1/120 s,
+E = 1e6 Pa, nu = 0.4, density 1000, bottom face pinned, seeded initial velocities, gravity -9.8 y.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+* value: whole-job vertex-iterations/s (all vertices x iterations x steps over all ranks / max over
+  ranks of the device-timed region), inputs resident in HBM, L2 flushed (256 MiB write) between
+  timed steps outside the timed events.
+* e2e: the same metric through the C ABI with host buffers: each step uploads positions and
+  velocities from pinned host memory, steps, and reads both back.
+* roofline: the colour-sweep kernel, timed live with a CUDA event pair around every launch (a
+  second timed pass); algorithmic bytes = 60 B per incident tet + 96 B per swept vertex.
+* cpu_baseline (rank 0, N = 1): the oracle's reference-cost restatement (literal 12x12 element
+  Hessian per incidence, energy every 10 iterations) on all host cores, one cube iteration per sample.
+* --impl reference: that CPU implementation alone (rank 0), each step one cube iteration.
+* N > 1 (torchrun): one replica of the cube per GPU ("replicas only": a single mesh does not
+  shard); no collective on the data path, barrier + max-over-ranks timing.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import signal
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "VBD vertex-iters/s on 1 B200 at stated tol; batched vs plain; adjoint/forward"
+UNIT = "vertex-iterations/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cube", type=int, default=64, help="cells per cube edge")
+    ap.add_argument("--iterations", type=int, default=50)
+    ap.add_argument("--lanes", type=int, default=None)
+    ap.add_argument("--layout", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(mesh, iters):
+    return {
+        "workload": f"cube{mesh.dims[0]} jittered Kuhn-split grid, VBDsolver::step x steps",
+        "vertices": mesh.num_verts,
+        "tets": mesh.num_tets,
+        "pinned": int(mesh.fixed.sum()),
+        "iterations_per_step": iters,
+        "dt": 1.0 / 120.0,
+        "chebyshev_rho": 0.9,
+        "E": 1e6,
+        "nu": 0.4,
+        "density": 1000.0,
+        "jitter": 0.2,
+        "seed": 1234,
+        "gravity": [0.0, -9.8, 0.0],
+        "l2": "flushed between timed steps (256 MiB write, outside the events)",
+    }
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def cpu_reference(mesh, iters_per_sample, samples, warmup=0):
+    """Times the oracle's reference-cost restatement on all host threads: (vertex-iters/s, cores)."""
+    from oracle import pyoracle as po
+
+    threads = max(1, os.cpu_count() or 1)
+    h = po.Handle(mesh, po.LITERAL_FULL12, threads)
+    s = 1.0 / 120.0
+    # computeTotalEnergy runs on every 10th iteration of the reference's loop (VBD.cpp:93-95); a
+    # sample of one iteration carries it on every 10th sample
+    k = 0
+    for _ in range(warmup):
+        h.step(1, s, iters_per_sample, (0.0, -9.8, 0.0), True, 0.9, energy=(k % 10 == 0))
+        k += iters_per_sample
+    times = []
+    for _ in range(samples):
+        t0 = time.perf_counter()
+        h.step(1, s, iters_per_sample, (0.0, -9.8, 0.0), True, 0.9, energy=(k % 10 == 0))
+        times.append(time.perf_counter() - t0)
+        k += iters_per_sample
+    h.close()
+    total = sum(times)
+    return mesh.num_verts * iters_per_sample * samples / total, threads, total
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+            self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{self.device_index}.csv")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.send_signal(signal.SIGTERM)
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5], f[6], f[7], f[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        sm = sorted(r[0] for r in rows)
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for name, val in zip(names, r[2:]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(r[1] for r in rows), "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def run_reference(args):
+    """--impl reference: the CPU implementation of the path, timed on the host (rank 0 only)."""
+    from vbd_tetmesh_b200 import meshgen
+
+    mesh = meshgen.cube(args.cube)
+    iters = 1
+    value, cores, total = cpu_reference(mesh, iters, args.steps, warmup=args.warmup)
+    cfg = workload_config(mesh, args.iterations)
+    cfg["sample"] = "each step = one colour sweep (1 VBD iteration) of the cube"
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": cfg,
+        "cpu_baseline": {
+            "value": value,
+            "unit": UNIT,
+            "cores": cores,
+            "kind": "port",
+            "sample": f"{args.steps} samples of 1 cube iteration (274,625 vertices), literal 12x12 element "
+                      "Hessian per incidence, energy every 10th iteration, OpenMP within each colour",
+        },
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+
+    import torch
+
+    from vbd_tetmesh_b200 import _capi, build_solver, meshgen
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        dist = dist_mod
+
+    mesh = meshgen.cube(args.cube)
+    iters = args.iterations
+    settings = meshgen.CUBE_SETTINGS
+    dt, rho, grav = settings["dt"], settings["rho"], settings["gravity"]
+    stream = torch.cuda.Stream(device=local)
+    solver = build_solver(mesh, device=local, stream=stream.cuda_stream, lanes=args.lanes, layout=args.layout)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            solver.step(dt, iters, grav, True, rho)
+        solver.sync()
+
+        # ---- timed region: device-resident steps, one event pair per step, L2 flushed between ----
+        clocks = ClockSampler(local)
+        barrier()
+        clocks.start()
+        launches0 = solver.kernel_launches()
+        ms_total = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            solver.step(dt, iters, grav, True, rho)
+            e1.record(stream)
+            e1.synchronize()
+            ms_total += e0.elapsed_time(e1)
+        barrier()
+        clock_info = clocks.stop()
+        launches = solver.kernel_launches() - launches0
+
+        # ---- kernel timing pass: event pair around every colour-sweep launch ----
+        solver.set_option(_capi.OPT_KERNEL_TIMING, 1)
+        solver.kernel_time(reset=True)
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            solver.step(dt, iters, grav, True, rho)
+        sweep_ms, sweep_launches, sweep_bytes = solver.kernel_time(reset=True)
+        solver.set_option(_capi.OPT_KERNEL_TIMING, 0)
+
+        # ---- e2e: host buffers through the C ABI ----
+        e2e_value = None
+        h2d = d2h = 2 * 12 * mesh.num_verts
+        if not args.no_e2e:
+            xh = torch.empty((mesh.num_verts, 3), dtype=torch.float32, pin_memory=True).numpy()
+            vh = torch.empty((mesh.num_verts, 3), dtype=torch.float32, pin_memory=True).numpy()
+            solver.get_positions(xh)
+            solver.get_velocities(vh)
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                solver.set_positions(xh)
+                solver.set_velocities(vh)
+                solver.step(dt, iters, grav, True, rho)
+                solver.get_positions(xh)
+                solver.get_velocities(vh)
+            e2e_s = time.perf_counter() - t0
+            barrier()
+
+    sing, nonf = solver.status()
+    t_max = torch.tensor([ms_total, e2e_s if not args.no_e2e else 0.0], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_max, e2e_max = float(t_max[0]), float(t_max[1])
+    units = float(mesh.num_verts) * iters * args.steps * world
+    value = units / (ms_max * 1e-3)
+    if not args.no_e2e:
+        e2e_value = units / e2e_max
+
+    peak, peak_kind = measured_peaks()
+    achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9 if sweep_ms > 0 else None
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "sweep_cube64_dram.txt")
+    if os.path.exists(prof):
+        for line in open(prof):
+            if line.startswith("dram_bytes_per_launch"):
+                traffic = float(line.split("=")[1].split()[0])
+    alg_bytes_per_vi = None
+    if sweep_launches:
+        alg_bytes_per_vi = sweep_bytes / (mesh.num_verts * iters * args.steps)
+
+    result = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": dict(workload_config(mesh, iters), parallelism=f"replicas x{world}" if world > 1 else "single GPU",
+                       lanes=solver.get_option(_capi.OPT_LANES), layout=solver.get_option(_capi.OPT_LAYOUT),
+                       graph=solver.get_option(_capi.OPT_GRAPH)),
+        "gpu_launches": int(launches),
+        "roofline": {
+            "bound": "hbm",
+            "kernel": "vbd::k_sweep (colour sweep)",
+            "achieved": achieved,
+            "peak": peak,
+            "peak_source": peak_kind,
+            "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None,
+            "traffic": traffic,
+            "sweep_launches_timed": int(sweep_launches),
+            "sweep_ms_avg": sweep_ms / sweep_launches if sweep_launches else None,
+            "alg_bytes_per_vertex_iteration": alg_bytes_per_vi,
+            "step_frac_of_roofline": (value / world) * (alg_bytes_per_vi or 0) / (peak * 1e9),
+        },
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "status": {"singular_skips": sing, "nonfinite": nonf},
+    }
+    if clock_info:
+        result["clocks"] = clock_info
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu_value, cores, total = cpu_reference(mesh, 1, 3)
+        result["cpu_baseline"] = {
+            "value": cpu_value,
+            "unit": UNIT,
+            "cores": cores,
+            "kind": "port",
+            "sample": "3 samples of 1 cube iteration (274,625 vertices), oracle reference-cost restatement: literal "
+                      "12x12 element Hessian per incidence, energy every 10th iteration, OpenMP within each colour",
+        }
+    solver.close()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

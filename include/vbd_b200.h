@@ -1,0 +1,208 @@
+/*
+ * vbd_b200.h -- C ABI of the B200 (sm_100a) Vertex Block Descent solver for tetrahedral
+ * Neo-Hookean elastodynamics.
+ *
+ * This is the drop-in boundary for the reference's VBD path (extinguish7/VBD_TetMesh).  Every
+ * entry point below names the reference interface it replaces (file:line in that project).
+ * Signatures use plain pointers and sizes only.  Layout conventions match the reference's own
+ * buffers:
+ *   - positions / velocities / inertia: float[3*N], xyz interleaved per vertex (the memory of an
+ *     Eigen 3xN column-major matrix, TetMesh::mVertPos.data(); VBD_GPU_Wrapper.cu:257);
+ *   - tets: int32[4*T], vertex ids per tet in the reference's local order (TetMesh::tets);
+ *   - Dm^-1: float[9*T], row-major per tet (VBD_GPU_Wrapper.cu:277-280);
+ *   - colour groups: CSR form of std::vector<std::vector<int>> -- offsets[C+1] and the
+ *     concatenated vertex ids (VBD_GPU_Wrapper.h:15).
+ * Any pointer argument for bulk data may be host memory (pageable or pinned) or device memory
+ * of the solver's device: copies use unified addressing.
+ *
+ * Error convention: every function returns a vbd_status; VBD_OK is 0.  vbd_last_error() returns
+ * the message of the last failing call on the calling thread.  A solver handle is not
+ * thread-safe: use one handle per host thread.
+ */
+#ifndef VBD_B200_H
+#define VBD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum vbd_status {
+    VBD_OK = 0,
+    VBD_ERR_INVALID_ARG = 1,   /* bad pointer, size, index or inconsistent input       */
+    VBD_ERR_CUDA = 2,          /* a CUDA runtime call failed                           */
+    VBD_ERR_STATE = 3,         /* call not valid in the handle's current state          */
+    VBD_ERR_NONFINITE = 4,     /* a NaN / Inf position was produced by the sweep        */
+    VBD_ERR_NO_DEVICE = 5,     /* no CUDA device, or the device is not sm_100           */
+    VBD_ERR_TIMEOUT = 6,       /* a bounded device-side wait gave up                   */
+    VBD_ERR_ALLOC = 7          /* device or host allocation failed                     */
+} vbd_status;
+
+typedef struct vbd_solver vbd_solver; /* opaque; owns all device memory of one mesh (or batch) */
+
+/* Library version, as 10000*major + 100*minor + patch. */
+int vbd_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* vbd_last_error(void);
+
+/* ------------------------------------------------------------------------------------------
+ * Host-side mesh set-up (no GPU needed).
+ * ------------------------------------------------------------------------------------------ */
+
+/* Greedy vertex colouring, bit-exact with GraphColoring::colorVertices (GraphColoring.cpp:28-66,
+ * neighbours from GraphColoring::getNeighbors :7-26): vertices in id order take the smallest
+ * colour unused by already-coloured vertices sharing a tet.  Writes colour_of[N] and the colour
+ * count.  If group_offsets (C+1 entries) and group_vertices (N entries) are non-null, also writes
+ * the colour groups in CSR form, each group in ascending vertex id (the reference's
+ * std::vector<std::vector<IdType>>).  Pass max_colours = capacity of group_offsets minus one. */
+int vbd_color_vertices(int32_t num_verts, int32_t num_tets, const int32_t* tets, int32_t* colour_of,
+                       int32_t* num_colours, int32_t max_colours, int32_t* group_offsets,
+                       int32_t* group_vertices);
+
+/* Rest volume and lumped mass, as TetMesh::initialize (TetMesh.h:249-265) and
+ * TetMesh::computeRestVolume (TetMesh.h:291-298): V_t = |e0.(e1 x e2)|/6, m_i += rho V_t / 4.
+ * Either output may be null. */
+int vbd_mesh_mass(int32_t num_verts, int32_t num_tets, const float* rest_xyz, const int32_t* tets,
+                  float density, float* vertex_mass, float* tet_rest_vol);
+
+/* Dm^-1 (row-major) and V0 = |d3.(d1 x d2)|/6 of each tet's rest shape, as
+ * VBDsolver::precomputeTetData (VBD.cpp:36-58) with ElasticEnergy::compute_Dm/compute_Volume
+ * (Energy.cpp:6-32). */
+int vbd_precompute_tets(int32_t num_verts, int32_t num_tets, const float* rest_xyz, const int32_t* tets,
+                        float* dm_inv, float* rest_vol);
+
+/* ------------------------------------------------------------------------------------------
+ * Solver handle (one GPU).  Replaces VBD::VBD_GPU_Solver (VBD_GPU_Wrapper.h:7-45) and the
+ * step loop of VBD::VBDsolver (VBD.cpp:60-112).
+ * ------------------------------------------------------------------------------------------ */
+
+/* Creates a handle on CUDA device `device`.  `cuda_stream` is a cudaStream_t (may be null: the
+ * handle then creates its own non-blocking stream).  Fails with VBD_ERR_NO_DEVICE if the device
+ * is absent or is not compute capability 10.0. */
+int vbd_solver_create(vbd_solver** out, int device, void* cuda_stream);
+
+/* Frees all device memory of the handle (VBD_GPU_Solver::~VBD_GPU_Solver,
+ * VBD_GPU_Wrapper.cu:373-382).  Null is accepted. */
+int vbd_solver_destroy(vbd_solver* s);
+
+/* Uploads one mesh (VBD_GPU_Solver::initFromCPU, VBD_GPU_Wrapper.cu:246-315).
+ *   positions[3N]       current positions x (TetMesh::mVertPos)
+ *   velocities[3N]      may be null (zero)           (TetMesh::mVelocity)
+ *   inertia[3N]         may be null (set to x)       (TetMesh::mInertia)
+ *   vertex_mass[N]      lumped masses                (TetMesh::vertexMass)
+ *   fixed[N]            1 = pinned                   (TetMesh::isFixed)
+ *   tets[4T]            vertex ids                   (TetMesh::tets)
+ *   num_colours, group_offsets[C+1], group_vertices[N]: colour groups (VBDsolver::vertexColors)
+ *   dm_inv[9T], rest_vol[T]                          (VBDsolver::tetDmInv / tetRestVolume)
+ *   tet_mu[T], tet_lambda[T]: per-tet Lame parameters (TetMesh::tetMu / tetLambda)
+ * Colour groups must partition the vertices and must be independent sets (no tet holds two
+ * vertices of one colour); tets must hold four distinct, in-range ids.  Calling it again
+ * replaces the previous mesh. */
+int vbd_solver_init(vbd_solver* s, int32_t num_verts, int32_t num_tets, const float* positions,
+                    const float* velocities, const float* inertia, const float* vertex_mass,
+                    const uint8_t* fixed, const int32_t* tets, int32_t num_colours,
+                    const int32_t* group_offsets, const int32_t* group_vertices, const float* dm_inv,
+                    const float* rest_vol, const float* tet_mu, const float* tet_lambda);
+
+/* Per-tet materials (TetMesh::tetMu / tetLambda, TetMesh.h:31-32); either pointer may be
+ * null to keep the current values. */
+int vbd_solver_set_materials(vbd_solver* s, const float* tet_mu, const float* tet_lambda);
+
+/* One (mu, lambda) for every tet: the reference's scalar VBDParams::mu / lambda
+ * (VBD.h:22-23, used at VBD.cpp:214-215) and the mu / lambda arguments of
+ * VBD_GPU_Solver::solveIteration / solveVBD (VBD_GPU_Wrapper.h:19,28). */
+int vbd_solver_set_uniform_material(vbd_solver* s, float mu, float lambda);
+
+/* State transfer.  set_inertia replaces VBD_GPU_Solver::updateInertiaFromCPU
+ * (VBD_GPU_Wrapper.cu:369-371); get_positions replaces copyPositionsToCPU (:364-366).  All
+ * arrays are float[3N] in the caller's vertex numbering.  Getters complete before returning. */
+int vbd_solver_set_positions(vbd_solver* s, const float* xyz);
+int vbd_solver_get_positions(vbd_solver* s, float* xyz);
+int vbd_solver_set_velocities(vbd_solver* s, const float* xyz);
+int vbd_solver_get_velocities(vbd_solver* s, float* xyz);
+int vbd_solver_set_inertia(vbd_solver* s, const float* xyz);
+int vbd_solver_get_inertia(vbd_solver* s, float* xyz);
+
+/* Initial guess of vbd_solver_solve. */
+typedef enum vbd_init_mode {
+    VBD_INIT_FROM_POSITIONS = 0, /* iterate from the current x (VBDsolver::step, VBD.cpp:76)   */
+    VBD_INIT_FROM_INERTIA = 1    /* iterate from x = y (VBD_GPU_Solver::solveVBD, :334)        */
+} vbd_init_mode;
+
+/* `iterations` Gauss-Seidel sweeps over the colour groups with the Chebyshev blend
+ * (VBD_GPU_Solver::solveVBD, VBD_GPU_Wrapper.cu:332-362; VBDsolver step loop VBD.cpp:75-96,
+ * getAcceleratorOmega :302-311).  Uses the inertia y already on the device.  Asynchronous. */
+int vbd_solver_solve(vbd_solver* s, int32_t iterations, float dt_sqr_reciprocal, int32_t use_acceleration,
+                     float rho, int32_t init_mode);
+
+/* One sweep without acceleration (VBD_GPU_Solver::solveIteration, VBD_GPU_Wrapper.cu:317-329).
+ * Asynchronous. */
+int vbd_solver_solve_iteration(vbd_solver* s, float dt_sqr_reciprocal);
+
+/* One time step on the GPU: for each of `substeps` sub-steps of h = dt/substeps, the inertial
+ * predictor (VBDsolver::forwardStep VBD.cpp:103-112: x_prev = x, v += h g, y = x + h v; y = x
+ * for pinned vertices), `iterations` sweeps with Chebyshev (VBD.cpp:75-96), and the velocity
+ * update v = (x - x_prev)/h * 0.999 (TetMesh::updateVelocity, TetMesh.h:305-311).  Replaces
+ * VBDsolver::step (VBD.cpp:60-101).  gravity is float[3].  Asynchronous. */
+int vbd_solver_step(vbd_solver* s, float dt, int32_t substeps, int32_t iterations, const float* gravity,
+                    int32_t use_acceleration, float rho);
+
+/* Waits for all work queued on the handle's stream and reports sticky device errors. */
+int vbd_solver_sync(vbd_solver* s);
+
+/* Energies (FP64 accumulation over the FP32 state).  Completes before returning.
+ *   VBD_ENERGY_IP:      incremental potential sum_i m_i/(2h^2)|x_i - y_i|^2 + sum_t V_t psi(F_t),
+ *                       psi = mu/2(|F|^2-3) - mu(J-1) + lambda/2 (J-1)^2 (the energy whose gradient
+ *                       the reference's force uses, Energy.cpp:97); h from `h`.
+ *   VBD_ENERGY_ELASTIC_LOGJ: VBDsolver::computeTotalEnergy (VBD.cpp:258-288 with
+ *                       NeoHookean::compute_Energy NeoHookean.cpp:6-20), J = |det F|; h ignored.
+ *   VBD_ENERGY_RESIDUAL: || m_i/h^2 (x_i - y_i) + dE/dx_i ||_2 over free vertices. */
+typedef enum vbd_energy_kind {
+    VBD_ENERGY_IP = 0,
+    VBD_ENERGY_ELASTIC_LOGJ = 1,
+    VBD_ENERGY_RESIDUAL = 2
+} vbd_energy_kind;
+int vbd_solver_energy(vbd_solver* s, int32_t kind, float h, double* out);
+
+/* Device-side counters since the last call with reset != 0: vertices whose 3x3 system failed
+ * the |det H| > 1e-8 guard and were left in place (VBD.cpp:141-156; the reference's GPU kernel
+ * printed a warning instead, VBD_GPU_Wrapper.cu:232), and whether a non-finite position was
+ * produced. */
+int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite, int32_t reset);
+
+/* Tuning knobs (all have measured defaults).
+ *   VBD_OPT_LANES:       threads cooperating on one vertex: 4, 8, 16 or 32
+ *   VBD_OPT_LAYOUT:      0 = tet records gathered through a per-vertex tet list,
+ *                        1 = incidence records streamed in colour order
+ *   VBD_OPT_GRAPH:       1 = replay a captured CUDA graph per step, 0 = direct launches
+ *   VBD_OPT_KERNEL_TIMING: 1 = launch directly and bracket every colour-sweep kernel with a CUDA
+ *                        event pair on the handle's stream (read with vbd_solver_kernel_time) */
+typedef enum vbd_option {
+    VBD_OPT_LANES = 0,
+    VBD_OPT_LAYOUT = 1,
+    VBD_OPT_GRAPH = 2,
+    VBD_OPT_KERNEL_TIMING = 3
+} vbd_option;
+int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value);
+int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value);
+
+/* Sizes of the uploaded mesh: vertices, tets, colours. */
+int vbd_solver_info(vbd_solver* s, int32_t* num_verts, int32_t* num_tets, int32_t* num_colours);
+
+/* Number of kernels this handle launched since creation (graph replays count their nodes). */
+int vbd_solver_kernel_launches(vbd_solver* s, int64_t* launches);
+
+/* With VBD_OPT_KERNEL_TIMING on: summed device time (ms) of the colour-sweep kernels timed since
+ * the last reset, their count, and the algorithmic bytes they moved (per free vertex swept:
+ * 60 B per incident tet -- tet id, 4 vertex ids, Dm^-1, V0 -- plus 96 B of vertex state).
+ * Completes the timed work first. */
+int vbd_solver_kernel_time(vbd_solver* s, double* sweep_ms, int64_t* sweep_launches, double* sweep_bytes,
+                           int32_t reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VBD_B200_H */

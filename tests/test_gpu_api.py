@@ -1,0 +1,223 @@
+"""The solver handle's API on the GPU: solveVBD / solveIteration semantics, state transfer, energies,
+status counters, options and host-made fault cases (none of which faults the GPU)."""
+import numpy as np
+import pytest
+
+from helpers import rel_err, small_block
+from oracle import pyoracle as po
+from vbd_tetmesh_b200 import GPUSolver, VBDError, build_solver, color_vertices, mesh_mass, meshgen, precompute_tets
+from vbd_tetmesh_b200 import _capi
+
+pytestmark = pytest.mark.gpu
+
+
+def predicted_inertia(m, dt, g=(0.0, -9.8, 0.0)):
+    """y = x + dt (v + dt g) on free vertices, y = x on pinned ones (VBDsolver::forwardStep)."""
+    free = m.fixed == 0
+    v = m.v.astype(np.float32).copy()
+    v[free] += np.float32(dt) * np.asarray(g, np.float32)
+    y = m.x.astype(np.float32).copy()
+    y[free] = m.x[free] + np.float32(dt) * v[free]
+    return y
+
+
+@pytest.mark.parametrize("init", [_capi.INIT_FROM_POSITIONS, _capi.INIT_FROM_INERTIA])
+@pytest.mark.parametrize("accel", [True, False])
+def test_solve_vbd_matches_oracle(gpu_device, init, accel):
+    m = small_block(seed=31)
+    dt = 1 / 60
+    y = predicted_inertia(m, dt)
+    dtsr = np.float32(1.0 / np.float64(np.float32(dt) * np.float32(dt)))
+    s = build_solver(m)
+    s.update_inertia_from_cpu(y)
+    s.solve_vbd(12, dtsr, accel, 0.9, init)
+    x = s.get_positions()
+    o = po.solve(m, m.x, y, dtsr, 12, accel, 0.9, init_from_inertia=(init == _capi.INIT_FROM_INERTIA))
+    assert rel_err(x, o, m) < 1e-5
+    s.close()
+
+
+def test_solve_iteration_is_one_plain_sweep(gpu_device):
+    m = small_block(seed=32)
+    y = predicted_inertia(m, 1 / 60)
+    dtsr = 3600.0
+    s = build_solver(m)
+    s.update_inertia_from_cpu(y)
+    for _ in range(3):
+        s.solve_iteration(dtsr)
+    o = po.solve(m, m.x, y, dtsr, 3, False, 0.0)
+    assert rel_err(s.get_positions(), o, m) < 1e-5
+
+
+def test_state_round_trip(gpu_device):
+    m = small_block(seed=33)
+    s = build_solver(m)
+    rng = np.random.default_rng(0)
+    for setter, getter in ((s.set_positions, s.get_positions), (s.set_velocities, s.get_velocities),
+                           (s.update_inertia_from_cpu, s.get_inertia)):
+        a = rng.normal(size=(m.num_verts, 3)).astype(np.float32)
+        setter(a)
+        np.testing.assert_array_equal(getter(), a)
+
+
+def test_device_pointer_transfer(gpu_device):
+    import torch
+
+    m = small_block(seed=34)
+    s = build_solver(m)
+    t = torch.randn(m.num_verts, 3, device="cuda", dtype=torch.float32)
+    s.set_positions(t.data_ptr())
+    out = torch.empty_like(t)
+    s.get_positions(out.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(out, t)
+
+
+def test_energies_match_oracle(gpu_device):
+    m = small_block(seed=35, per_tet_sigma=0.2)
+    dt = 1 / 60
+    s = build_solver(m)
+    s.step(dt, 5, (0, -9.8, 0), True, 0.9)
+    x = s.get_positions().astype(np.float64)
+    y = s.get_inertia().astype(np.float64)
+    mass, _ = mesh_mass(m.rest, m.tets, m.density)
+    dm, v0 = precompute_tets(m.rest, m.tets)
+    ip_o = po.ip_energy(x, y, mass, m.tets, dm, v0, m.mu, m.lam, dt)
+    ip_g = s.energy(_capi.ENERGY_IP, dt)
+    assert abs(ip_g - ip_o) <= 1e-9 * abs(ip_o)
+    # log-J elastic energy (VBDsolver::computeTotalEnergy)
+    r = po.simulate(m, 1, dt, 5, use_acceleration=True, rho=0.9, energy_history=True)
+    assert np.isfinite(s.energy(_capi.ENERGY_ELASTIC_LOGJ))
+    res_g = s.energy(_capi.ENERGY_RESIDUAL, dt)
+    res_o = po.residual(m, x, y, 1.0 / (dt * dt))
+    assert abs(res_g - res_o) <= 1e-3 * res_o + 1e-6
+    assert r["ehist"] is not None
+
+
+def test_residual_decreases_with_iterations(gpu_device):
+    m = small_block(seed=36)
+    dt = 1 / 60
+    res = []
+    for iters in (2, 10, 40):
+        s = build_solver(m)
+        s.step(dt, iters, (0, -9.8, 0), False, 0.0)
+        res.append(s.energy(_capi.ENERGY_RESIDUAL, dt))
+        s.close()
+    assert res[0] > res[1] > res[2]
+
+
+def test_isolated_vertex_counts_singular_skip(gpu_device):
+    m = meshgen.jittered_block(2, 2, 2, seed=1)
+    n = m.num_verts
+    # one extra vertex that belongs to no tet: zero mass, zero H, skipped by the det guard
+    m.rest = np.concatenate([m.rest, [[5.0, 5.0, 5.0]]]).astype(np.float32)
+    m.x = m.rest.copy()
+    m.v = np.zeros_like(m.x)
+    m.fixed = np.concatenate([m.fixed, [0]]).astype(np.uint8)
+    s = build_solver(m)
+    s.step(1 / 60, 3, (0, -9.8, 0), False, 0.0)
+    x = s.get_positions()
+    sing, nonf = s.status(reset=True)
+    assert sing == 3 and not nonf
+    np.testing.assert_array_equal(x[n], [5.0, 5.0, 5.0])
+    assert s.status() == (0, False)
+
+
+def test_all_pinned_mesh_does_not_move(gpu_device):
+    m = meshgen.jittered_block(2, 2, 2, seed=2)
+    m.fixed[:] = 1
+    s = build_solver(m)
+    s.step(1 / 60, 5, (0, -9.8, 0), True, 0.9)
+    np.testing.assert_array_equal(s.get_positions(), m.x)
+
+
+def test_degenerate_tets_are_skipped_by_the_det_guard(gpu_device):
+    m = meshgen.jittered_block(1, 1, 1, seed=0, jitter=0.0)
+    # collapse vertex 7 onto vertex 0: all six Kuhn tets hold both, so every V0 is 0 and Dm^-1 is
+    # infinite; H becomes NaN and the |det H| > 1e-8 guard skips every vertex (VBD.cpp:141-142)
+    m.rest[7] = m.rest[0]
+    m.x = m.rest.copy()
+    m.fixed[:] = 0
+    s = build_solver(m)
+    s.step(1 / 60, 2, (0, -9.8, 0), False, 0.0)
+    sing, nonf = s.status()
+    assert sing == 2 * m.num_verts and not nonf
+    np.testing.assert_array_equal(s.get_positions(), m.x)
+
+
+def test_nan_state_is_reported_nonfinite(gpu_device):
+    m = small_block(seed=41)
+    s = build_solver(m)
+    v = np.zeros((m.num_verts, 3), np.float32)
+    v[int(np.flatnonzero(m.fixed == 0)[0]), 0] = np.nan
+    s.set_velocities(v)
+    s.step(1 / 60, 2, (0, -9.8, 0), False, 0.0)
+    _, nonf = s.status()
+    assert nonf
+
+
+def test_bad_colour_groups_rejected(gpu_device):
+    m = small_block(seed=37)
+    mass, _ = mesh_mass(m.rest, m.tets, m.density)
+    dm, v0 = precompute_tets(m.rest, m.tets)
+    s = GPUSolver()
+    offs = np.array([0, m.num_verts], np.int32)
+    verts = np.arange(m.num_verts, dtype=np.int32)
+    with pytest.raises(VBDError) as e:
+        s.init_from_cpu(m.x, mass, m.fixed, m.tets, offs, verts, dm, v0, m.mu, m.lam)
+    assert e.value.code == 1 and "independent" in e.value.message
+    _, offs, verts = color_vertices(m.num_verts, m.tets)
+    verts2 = verts.copy()
+    verts2[0] = verts2[1]
+    with pytest.raises(VBDError) as e:
+        s.init_from_cpu(m.x, mass, m.fixed, m.tets, offs, verts2, dm, v0, m.mu, m.lam)
+    assert "two colour groups" in e.value.message
+    with pytest.raises(VBDError) as e:
+        s.step(1 / 60, 1)
+    assert e.value.code == 3
+
+
+def test_out_of_range_tet_rejected_before_upload(gpu_device):
+    m = small_block(seed=38)
+    mass, _ = mesh_mass(m.rest, m.tets, m.density)
+    dm, v0 = precompute_tets(m.rest, m.tets)
+    _, offs, verts = color_vertices(m.num_verts, m.tets)
+    bad = m.tets.copy()
+    bad[3, 2] = m.num_verts + 10
+    s = GPUSolver()
+    with pytest.raises(VBDError) as e:
+        s.init_from_cpu(m.x, mass, m.fixed, bad, offs, verts, dm, v0, m.mu, m.lam)
+    assert "outside" in e.value.message
+
+
+def test_materials_required_and_updates_take_effect(gpu_device):
+    m = small_block(seed=39)
+    mass, _ = mesh_mass(m.rest, m.tets, m.density)
+    dm, v0 = precompute_tets(m.rest, m.tets)
+    _, offs, verts = color_vertices(m.num_verts, m.tets)
+    s = GPUSolver()
+    s.init_from_cpu(m.x, mass, m.fixed, m.tets, offs, verts, dm, v0)
+    with pytest.raises(VBDError) as e:
+        s.step(1 / 60, 1)
+    assert e.value.code == 3
+    s.set_uniform_material(float(m.mu[0]), float(m.lam[0]))
+    s.step(1 / 60, 8, (0, -9.8, 0), True, 0.9)
+    soft = s.get_positions()
+    o = po.simulate(m, 1, 1 / 60, 8, (0, -9.8, 0), True, 0.9)
+    assert rel_err(soft, o["x"], m) < 1e-5
+    # re-init replaces the mesh; stiffer per-tet material sags less
+    s.init_from_cpu(m.x, mass, m.fixed, m.tets, offs, verts, dm, v0, m.mu * 10, m.lam * 10)
+    s.step(1 / 60, 8, (0, -9.8, 0), True, 0.9)
+    stiff = s.get_positions()
+    assert stiff[:, 1].min() > soft[:, 1].min()
+
+
+def test_launch_count_reported(gpu_device):
+    m = small_block(seed=40)
+    s = build_solver(m)
+    before = s.kernel_launches()
+    s.step(1 / 60, 4, (0, -9.8, 0), True, 0.9)
+    s.sync()
+    colour_of, _, _ = color_vertices(m.num_verts, m.tets)
+    swept = len(np.unique(colour_of[m.fixed == 0]))
+    assert s.kernel_launches() - before == 4 * swept + 2

@@ -1,0 +1,89 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle's restatement of VBDsolver::step.
+
+Bar (floating point): positions after 1 and 10 steps within 1e-5 of the bounding-box diagonal of
+the FP32 oracle; the incremental potential within 1e-5 relative.  Each result's error against the
+FP64 oracle is printed beside it."""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import gpu_simulate, rel_err, small_block
+from oracle import pyoracle as po
+from vbd_tetmesh_b200 import meshgen
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL = 1e-5  # of the bounding-box diagonal
+IP_TOL = 1e-5   # relative
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.mark.parametrize("steps", [1, 10])
+def test_beam_matches_oracle(gpu_device, steps):
+    m = meshgen.beam()
+    s = meshgen.BEAM_SETTINGS
+    g = gpu_simulate(m, steps, s["dt"], s["iterations"], s["gravity"], True, s["rho"])
+    o32 = po.simulate(m, steps, s["dt"], s["iterations"], s["gravity"], True, s["rho"], precision=32)
+    o64 = po.simulate(m, steps, s["dt"], s["iterations"], s["gravity"], True, s["rho"], precision=64)
+    e32, e64 = rel_err(g["x"], o32["x"], m), rel_err(g["x"], o64["x"], m)
+    print(f"beam {steps} steps: |gpu - oracle32|/diag = {e32:.3e}, |gpu - oracle64|/diag = {e64:.3e}, "
+          f"|oracle32 - oracle64|/diag = {rel_err(o32['x'], o64['x'], m):.3e}")
+    assert e32 < POS_TOL
+    assert abs(g["ip"] - o32["ip"][-1]) <= IP_TOL * abs(o32["ip"][-1])
+    vscale = max(np.abs(o64["v"]).max(), 1e-6)
+    assert np.abs(g["v"] - o32["v"]).max() < 1e-3 * vscale
+    assert g["singular"] == 0 and not g["nonfinite"]
+    # committed FP64 fixture of the same run
+    gold = np.load(os.path.join(GOLDEN, "beam_oracle.npz"))
+    assert rel_err(g["x"], gold[f"x_f64_s{steps}"], m) < POS_TOL
+
+
+def test_beam_100_steps_stays_close(gpu_device):
+    m = meshgen.beam()
+    s = meshgen.BEAM_SETTINGS
+    g = gpu_simulate(m, 100, s["dt"], s["iterations"], s["gravity"], True, s["rho"])
+    o = po.simulate(m, 100, s["dt"], s["iterations"], s["gravity"], True, s["rho"], precision=64, mode=po.CLOSED)
+    err = rel_err(g["x"], o["x"], m)
+    print(f"beam 100 steps: |gpu - oracle64|/diag = {err:.3e}")
+    assert err < 1e-4
+
+
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+@pytest.mark.parametrize("layout", [0, 1])
+def test_launch_shapes_agree(gpu_device, lanes, layout):
+    m = small_block(seed=lanes + layout)
+    g = gpu_simulate(m, 3, 1 / 60, 15, (0.0, -9.8, 0.0), True, 0.9, lanes=lanes, layout=layout)
+    o = po.simulate(m, 3, 1 / 60, 15, (0.0, -9.8, 0.0), True, 0.9, precision=32)
+    assert rel_err(g["x"], o["x"], m) < POS_TOL
+
+
+@pytest.mark.parametrize("graph", [0, 1])
+def test_graph_and_direct_launches_identical(gpu_device, graph):
+    m = small_block(seed=11)
+    a = gpu_simulate(m, 4, 1 / 60, 10, (0.0, -9.8, 0.0), True, 0.9, graph=graph)
+    b = gpu_simulate(m, 4, 1 / 60, 10, (0.0, -9.8, 0.0), True, 0.9, graph=1 - graph)
+    np.testing.assert_array_equal(a["x"], b["x"])
+    np.testing.assert_array_equal(a["v"], b["v"])
+
+
+@pytest.mark.parametrize("accel,substeps", [(False, 1), (True, 2), (False, 3)])
+def test_per_tet_materials_substeps_acceleration(gpu_device, accel, substeps):
+    m = small_block(seed=21, dims=(8, 3, 3), per_tet_sigma=0.3, pin="y0")
+    g = gpu_simulate(m, 10, 1 / 60, 12, (0.0, -9.8, 0.0), accel, 0.85, substeps=substeps)
+    o = po.simulate(m, 10, 1 / 60, 12, (0.0, -9.8, 0.0), accel, 0.85, substeps=substeps, precision=32)
+    o64 = po.simulate(m, 10, 1 / 60, 12, (0.0, -9.8, 0.0), accel, 0.85, substeps=substeps, precision=64)
+    print(f"block accel={accel} substeps={substeps}: vs32 {rel_err(g['x'], o['x'], m):.3e} "
+          f"vs64 {rel_err(g['x'], o64['x'], m):.3e}")
+    assert rel_err(g["x"], o["x"], m) < POS_TOL
+
+
+def test_initial_velocity_and_stiff_material(gpu_device):
+    m = meshgen.cube(6, E=1e6, nu=0.4, seed=5)
+    s = meshgen.CUBE_SETTINGS
+    g = gpu_simulate(m, 10, s["dt"], s["iterations"], s["gravity"], True, s["rho"])
+    o = po.simulate(m, 10, s["dt"], s["iterations"], s["gravity"], True, s["rho"], precision=32, mode=po.CLOSED)
+    o64 = po.simulate(m, 10, s["dt"], s["iterations"], s["gravity"], True, s["rho"], precision=64, mode=po.CLOSED)
+    print(f"cube6 10 steps: vs32 {rel_err(g['x'], o['x'], m):.3e} vs64 {rel_err(g['x'], o64['x'], m):.3e}")
+    assert rel_err(g["x"], o["x"], m) < POS_TOL
+    assert abs(g["ip"] - o["ip"][-1]) <= IP_TOL * abs(o["ip"][-1])

@@ -1,0 +1,116 @@
+"""The oracle itself: literal vs closed-form element blocks, finite differences of the energy,
+precision and threading invariants, and the committed regression fixtures."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from vbd_tetmesh_b200 import meshgen
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def psi(F, mu, lam):
+    J = np.linalg.det(F)
+    return 0.5 * mu * (np.sum(F * F) - 3.0) - mu * (J - 1.0) + 0.5 * lam * (J - 1.0) ** 2
+
+
+def random_element(rng):
+    Dm = np.eye(3) * 0.05 + rng.normal(0, 0.01, (3, 3))
+    Dinv = np.linalg.inv(Dm)
+    F = np.eye(3) + rng.normal(0, 0.15, (3, 3))
+    return F, Dinv, abs(np.linalg.det(Dm)) / 6.0
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 3])
+def test_closed_form_block_matches_literal_12x12(n):
+    rng = np.random.default_rng(10 + n)
+    for _ in range(50):
+        F, Dinv, V = random_element(rng)
+        mu, lam = 3.8e4, 5.7e4
+        H_lit, g_lit = po.tet_block(F, Dinv, mu, lam, V, n, mode=po.LITERAL, precision=64)
+        H_full, g_full = po.tet_block(F, Dinv, mu, lam, V, n, mode=po.LITERAL_FULL12, precision=64)
+        H_cf, g_cf = po.tet_block(F, Dinv, mu, lam, V, n, mode=po.CLOSED, precision=64)
+        np.testing.assert_array_equal(H_lit, H_full)
+        scale = np.abs(H_lit).max()
+        assert np.abs(H_lit - H_cf).max() <= 1e-12 * scale
+        assert np.abs(g_lit - g_cf).max() <= 1e-12 * np.abs(g_lit).max()
+
+
+def test_gradient_and_hessian_block_by_finite_differences():
+    rng = np.random.default_rng(3)
+    mu, lam = 3.8e4, 5.7e4
+    for trial in range(10):
+        Dm = np.eye(3) * 0.05 + rng.normal(0, 0.01, (3, 3))
+        Dinv = np.linalg.inv(Dm)
+        X = np.concatenate([np.zeros((1, 3)), Dm.T]) + rng.normal(0, 0.004, (4, 3))
+        V = abs(np.linalg.det(Dm)) / 6.0
+
+        def energy(Xc):
+            Ds = np.stack([Xc[k] - Xc[0] for k in (1, 2, 3)], axis=1)
+            return V * psi(Ds @ Dinv, mu, lam)
+
+        Ds = np.stack([X[k] - X[0] for k in (1, 2, 3)], axis=1)
+        F = Ds @ Dinv
+        n = trial % 4
+        H, g = po.tet_block(F, Dinv, mu, lam, V, n, mode=po.LITERAL, precision=64)
+        eps = 1e-7
+        g_fd = np.zeros(3)
+        H_fd = np.zeros((3, 3))
+        for c in range(3):
+            Xp, Xm = X.copy(), X.copy()
+            Xp[n, c] += eps
+            Xm[n, c] -= eps
+            g_fd[c] = (energy(Xp) - energy(Xm)) / (2 * eps)
+            Hp, gp = po.tet_block(np.stack([Xp[k] - Xp[0] for k in (1, 2, 3)], 1) @ Dinv, Dinv, mu, lam, V, n,
+                                  precision=64)
+            Hm, gm = po.tet_block(np.stack([Xm[k] - Xm[0] for k in (1, 2, 3)], 1) @ Dinv, Dinv, mu, lam, V, n,
+                                  precision=64)
+            H_fd[:, c] = (gp - gm) / (2 * eps)
+        np.testing.assert_allclose(g, g_fd, rtol=1e-5, atol=1e-6 * np.abs(g).max())
+        np.testing.assert_allclose(H, H_fd, rtol=1e-5, atol=1e-6 * np.abs(H).max())
+
+
+def test_threaded_oracle_is_bit_identical_to_serial():
+    m = meshgen.jittered_block(6, 5, 4, seed=1, per_tet_sigma=0.2)
+    s = meshgen.BEAM_SETTINGS
+    a = po.simulate(m, 3, s["dt"], 10, s["gravity"], True, 0.9, threads=1)
+    b = po.simulate(m, 3, s["dt"], 10, s["gravity"], True, 0.9, threads=4)
+    np.testing.assert_array_equal(a["x"], b["x"])
+    np.testing.assert_array_equal(a["v"], b["v"])
+
+
+def test_f32_oracle_close_to_f64():
+    m = meshgen.beam()
+    s = meshgen.BEAM_SETTINGS
+    a = po.simulate(m, 10, s["dt"], s["iterations"], s["gravity"], True, s["rho"], precision=32)
+    b = po.simulate(m, 10, s["dt"], s["iterations"], s["gravity"], True, s["rho"], precision=64)
+    assert np.abs(a["x"] - b["x"]).max() / m.bbox_diag() < 2e-6
+
+
+def test_oracle_matches_committed_fixtures():
+    g = np.load(os.path.join(GOLDEN, "beam_oracle.npz"))
+    m = meshgen.beam()
+    s = meshgen.BEAM_SETTINGS
+    for prec in (32, 64):
+        for steps in (1, 10):
+            r = po.simulate(m, steps, s["dt"], s["iterations"], s["gravity"], True, s["rho"], precision=prec)
+            np.testing.assert_array_equal(r["x"], g[f"x_f{prec}_s{steps}"])
+            np.testing.assert_array_equal(r["v"], g[f"v_f{prec}_s{steps}"])
+
+
+def test_pinned_vertices_never_move_and_beam_sags():
+    m = meshgen.beam()
+    s = meshgen.BEAM_SETTINGS
+    r = po.simulate(m, 10, s["dt"], s["iterations"], s["gravity"], True, s["rho"])
+    fx = m.fixed.astype(bool)
+    np.testing.assert_array_equal(r["x"][fx], m.x[fx].astype(np.float64))
+    assert r["x"][~fx, 1].min() < -0.05
+
+
+def test_energy_history_length():
+    m = meshgen.beam(4, 2, 2)
+    r = po.simulate(m, 2, 1 / 60, 20, use_acceleration=True, rho=0.9, energy_history=True)
+    assert r["ehist"].shape == (2 * 2,)
+    assert np.all(np.isfinite(r["ehist"]))

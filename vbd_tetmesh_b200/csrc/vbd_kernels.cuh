@@ -1,0 +1,467 @@
+// Device code of the VBD solver: data layout, per-incidence element math and the kernels.
+//
+// Layout in HBM (one mesh, or a batch of meshes concatenated):
+//   Vertices are renumbered "internally": the free vertices of colour 0, then of colour 1, ...,
+//   then every pinned vertex.  Each colour is therefore one contiguous id range and a sweep
+//   kernel reads and writes its own vertices' state fully coalesced.
+//   float4 x[2][N]   positions, ping-pong pair (w unused)      -- Chebyshev needs x~ and x^(k)
+//   float4 pp[N]     position before the previous sweep       -- VBDsolver::prevPrevPos
+//   float4 y[N]      inertial target, w = lumped mass         -- TetMesh::mInertia / vertexMass
+//   float4 v[N], xprev[N]                                       -- TetMesh::mVelocity / mVertPrevPos
+//   TetRec rec[T]    64 B per tet, in the caller's tet order:  four internal vertex ids, Dm^-1
+//                    row-major, V0, mu, lambda
+//   int inc_off[N+1], inc_tet[4T]: per free vertex, its incident tets in ascending tet id
+//                    (TetMesh::vertAdjacentTets); pinned vertices own none.
+//   TetRec irec[4T]  (optional "streamed" layout) rec[inc_tet[j]] copied in incidence order, so a
+//                    sweep reads its element data as one sequential stream.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace vbd {
+
+struct __align__(16) TetRec {
+    int4 ids;   // internal vertex ids in the tet's local order
+    float4 a;   // Dm^-1: (0,0) (0,1) (0,2) (1,0)
+    float4 b;   //        (1,1) (1,2) (2,0) (2,1)
+    float4 c;   //        (2,2), V0, mu, lambda
+};
+static_assert(sizeof(TetRec) == 64, "TetRec must be 64 bytes");
+
+enum StatusSlot { ST_SINGULAR = 0, ST_NONFINITE = 1, ST_SLOTS = 4 };
+
+struct SweepParams {
+    float4* x;                 // positions being swept in place (Gauss-Seidel)
+    float4* xnext;             // receives the Chebyshev-blended position (ACCEL)
+    float4* pp;                // position before the previous sweep
+    const float4* y;           // inertial target, w = mass
+    const int* inc_off;
+    const int* inc_tet;
+    const TetRec* rec;
+    const TetRec* irec;
+    unsigned long long* status;
+    int v_begin, v_end;
+    float dtsr;                // 1/h^2
+    float omega;
+};
+
+__device__ __forceinline__ TetRec load_rec(const TetRec* p) {
+    TetRec r;
+    const int4* q = reinterpret_cast<const int4*>(p);
+    r.ids = __ldg(q);
+    int4 t;
+    t = __ldg(q + 1);
+    r.a = make_float4(__int_as_float(t.x), __int_as_float(t.y), __int_as_float(t.z), __int_as_float(t.w));
+    t = __ldg(q + 2);
+    r.b = make_float4(__int_as_float(t.x), __int_as_float(t.y), __int_as_float(t.z), __int_as_float(t.w));
+    t = __ldg(q + 3);
+    r.c = make_float4(__int_as_float(t.x), __int_as_float(t.y), __int_as_float(t.z), __int_as_float(t.w));
+    return r;
+}
+
+// Accumulators of one vertex's elastic terms: the symmetric 3x3 Hessian block (6 entries) and
+// the gradient (3 entries).
+struct Acc {
+    float h00, h01, h02, h11, h12, h22, g0, g1, g2;
+    __device__ __forceinline__ void zero() { h00 = h01 = h02 = h11 = h12 = h22 = g0 = g1 = g2 = 0.f; }
+};
+
+// Element contribution of tet `r` to vertex `v` (internal id), whose position is `xi`.
+// Neighbour positions are gathered from X, which this kernel never writes at those ids (they are
+// of another colour).  Follows ElasticEnergy::compute_Hessian_and_Gradient (Energy.cpp:90-158)
+// as used by VBDsolver::computeTetContribution (VBD.cpp:205-256):
+//   Ds = [x1-x0, x2-x0, x3-x0], F = Ds Dm^-1, J = det F, C = cof F,
+//   P = mu (F - C) + lambda (J - 1) C, q = row n of Ps Dm^-1,
+//   gradient  g_n  = V P q,
+//   Hessian   H_nn = V (mu |q|^2 I + lambda (C q)(C q)^T)   -- the (n,n) block of the literal
+//   12x12 assembly; the cofactor-derivative terms vanish in that block because dC_ij/dF_kl is
+//   antisymmetric in (j,l) and is contracted with the symmetric q q^T.
+template <bool WANT_H>
+__device__ __forceinline__ void tet_contrib(const TetRec& r, int v, float4 xi, const float4* __restrict__ X,
+                                            Acc& acc) {
+    const int i0 = r.ids.x, i1 = r.ids.y, i2 = r.ids.z, i3 = r.ids.w;
+    const float4 p0 = (i0 == v) ? xi : __ldg(X + i0);
+    const float4 p1 = (i1 == v) ? xi : __ldg(X + i1);
+    const float4 p2 = (i2 == v) ? xi : __ldg(X + i2);
+    const float4 p3 = (i3 == v) ? xi : __ldg(X + i3);
+    const int n = (i0 == v) ? 0 : (i1 == v) ? 1 : (i2 == v) ? 2 : 3;
+
+    const float D00 = r.a.x, D01 = r.a.y, D02 = r.a.z, D10 = r.a.w;
+    const float D11 = r.b.x, D12 = r.b.y, D20 = r.b.z, D21 = r.b.w;
+    const float D22 = r.c.x, V0 = r.c.y, mu = r.c.z, lam = r.c.w;
+
+    const float e1x = p1.x - p0.x, e1y = p1.y - p0.y, e1z = p1.z - p0.z;
+    const float e2x = p2.x - p0.x, e2y = p2.y - p0.y, e2z = p2.z - p0.z;
+    const float e3x = p3.x - p0.x, e3y = p3.y - p0.y, e3z = p3.z - p0.z;
+
+    // F = Ds * Dm^-1
+    const float F00 = e1x * D00 + e2x * D10 + e3x * D20;
+    const float F01 = e1x * D01 + e2x * D11 + e3x * D21;
+    const float F02 = e1x * D02 + e2x * D12 + e3x * D22;
+    const float F10 = e1y * D00 + e2y * D10 + e3y * D20;
+    const float F11 = e1y * D01 + e2y * D11 + e3y * D21;
+    const float F12 = e1y * D02 + e2y * D12 + e3y * D22;
+    const float F20 = e1z * D00 + e2z * D10 + e3z * D20;
+    const float F21 = e1z * D01 + e2z * D11 + e3z * D21;
+    const float F22 = e1z * D02 + e2z * D12 + e3z * D22;
+
+    // cofactor matrix
+    const float C00 = F11 * F22 - F12 * F21;
+    const float C01 = F12 * F20 - F10 * F22;
+    const float C02 = F10 * F21 - F11 * F20;
+    const float C10 = F21 * F02 - F22 * F01;
+    const float C11 = F22 * F00 - F20 * F02;
+    const float C12 = F20 * F01 - F21 * F00;
+    const float C20 = F01 * F12 - F02 * F11;
+    const float C21 = F02 * F10 - F00 * F12;
+    const float C22 = F00 * F11 - F01 * F10;
+    const float J = F00 * C00 + F01 * C01 + F02 * C02;
+    const float s = lam * (J - 1.0f);
+
+    // q = row n of Ps * Dm^-1
+    float qx, qy, qz;
+    if (n == 0) {
+        qx = -D00 - D10 - D20;
+        qy = -D01 - D11 - D21;
+        qz = -D02 - D12 - D22;
+    } else if (n == 1) {
+        qx = D00; qy = D01; qz = D02;
+    } else if (n == 2) {
+        qx = D10; qy = D11; qz = D12;
+    } else {
+        qx = D20; qy = D21; qz = D22;
+    }
+
+    const float Fq0 = F00 * qx + F01 * qy + F02 * qz;
+    const float Fq1 = F10 * qx + F11 * qy + F12 * qz;
+    const float Fq2 = F20 * qx + F21 * qy + F22 * qz;
+    const float Cq0 = C00 * qx + C01 * qy + C02 * qz;
+    const float Cq1 = C10 * qx + C11 * qy + C12 * qz;
+    const float Cq2 = C20 * qx + C21 * qy + C22 * qz;
+
+    acc.g0 += V0 * (mu * (Fq0 - Cq0) + s * Cq0);
+    acc.g1 += V0 * (mu * (Fq1 - Cq1) + s * Cq1);
+    acc.g2 += V0 * (mu * (Fq2 - Cq2) + s * Cq2);
+    if (WANT_H) {
+        const float a = V0 * mu * (qx * qx + qy * qy + qz * qz);
+        const float b = V0 * lam;
+        const float b0 = b * Cq0, b1 = b * Cq1, b2 = b * Cq2;
+        acc.h00 += a + b0 * Cq0;
+        acc.h01 += b0 * Cq1;
+        acc.h02 += b0 * Cq2;
+        acc.h11 += a + b1 * Cq1;
+        acc.h12 += b1 * Cq2;
+        acc.h22 += a + b2 * Cq2;
+    }
+}
+
+template <int LANES>
+__device__ __forceinline__ void group_reduce(Acc& a) {
+#pragma unroll
+    for (int o = LANES / 2; o > 0; o >>= 1) {
+        a.h00 += __shfl_xor_sync(0xffffffffu, a.h00, o);
+        a.h01 += __shfl_xor_sync(0xffffffffu, a.h01, o);
+        a.h02 += __shfl_xor_sync(0xffffffffu, a.h02, o);
+        a.h11 += __shfl_xor_sync(0xffffffffu, a.h11, o);
+        a.h12 += __shfl_xor_sync(0xffffffffu, a.h12, o);
+        a.h22 += __shfl_xor_sync(0xffffffffu, a.h22, o);
+        a.g0 += __shfl_xor_sync(0xffffffffu, a.g0, o);
+        a.g1 += __shfl_xor_sync(0xffffffffu, a.g1, o);
+        a.g2 += __shfl_xor_sync(0xffffffffu, a.g2, o);
+    }
+}
+
+// One colour of one Gauss-Seidel sweep (VBDsolver::solve, VBD.cpp:114-158, and solveVertex
+// :160-203): LANES threads per vertex split its incident tets, reduce with warp shuffles, and
+// the group's first lane solves (m/h^2 I + sum H_nn) dx = m/h^2 (y - x) - sum g_n with the
+// adjugate formula behind the |det| > 1e-8 guard (VBD.cpp:141-152, Types.h:85-112).
+//   STREAM : element records read from the incidence-ordered copy instead of through inc_tet
+//   ACCEL  : also write x^(k) = omega (x~ - pp) + pp to xnext (VBD.cpp:290-300)
+//   KEEP_PP: store the pre-sweep position into pp (VBD.cpp:78,89)
+template <int LANES, bool STREAM, bool ACCEL, bool KEEP_PP>
+__global__ void __launch_bounds__(256) k_sweep(SweepParams p) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & (LANES - 1);
+    const int v = p.v_begin + t / LANES;
+    const bool active = v < p.v_end;
+    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
+    int j0 = 0, j1 = 0;
+    if (active) {
+        xi = p.x[v];
+        j0 = __ldg(p.inc_off + v);
+        j1 = __ldg(p.inc_off + v + 1);
+    }
+    Acc acc;
+    acc.zero();
+    for (int j = j0 + lane; j < j1; j += LANES) {
+        const TetRec r = STREAM ? load_rec(p.irec + j) : load_rec(p.rec + __ldg(p.inc_tet + j));
+        tet_contrib<true>(r, v, xi, p.x, acc);
+    }
+    group_reduce<LANES>(acc);
+    if (!active || lane != 0) return;
+
+    const float4 yi = p.y[v];
+    const float cm = yi.w * p.dtsr;
+    const float H00 = cm + acc.h00, H01 = acc.h01, H02 = acc.h02;
+    const float H11 = cm + acc.h11, H12 = acc.h12, H22 = cm + acc.h22;
+    const float f0 = (yi.w * (yi.x - xi.x)) * p.dtsr - acc.g0;
+    const float f1 = (yi.w * (yi.y - xi.y)) * p.dtsr - acc.g1;
+    const float f2 = (yi.w * (yi.z - xi.z)) * p.dtsr - acc.g2;
+    // adjugate of the symmetric H
+    const float A00 = H11 * H22 - H12 * H12;
+    const float A01 = H02 * H12 - H01 * H22;
+    const float A02 = H01 * H12 - H02 * H11;
+    const float A11 = H00 * H22 - H02 * H02;
+    const float A12 = H02 * H01 - H00 * H12;
+    const float A22 = H00 * H11 - H01 * H01;
+    const float det = H00 * A00 + H01 * A01 + H02 * A02;
+    float4 xn = xi;
+    if (fabsf(det) > 1e-8f) {
+        const float inv = 1.0f / det;
+        xn.x = xi.x + inv * (A00 * f0 + A01 * f1 + A02 * f2);
+        xn.y = xi.y + inv * (A01 * f0 + A11 * f1 + A12 * f2);
+        xn.z = xi.z + inv * (A02 * f0 + A12 * f1 + A22 * f2);
+    } else {
+        atomicAdd(p.status + ST_SINGULAR, 1ull);
+    }
+    if (!(isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z))) p.status[ST_NONFINITE] = 1ull;
+    p.x[v] = xn;
+    if (ACCEL) {
+        const float4 q = p.pp[v];
+        float4 xa;
+        xa.x = p.omega * (xn.x - q.x) + q.x;
+        xa.y = p.omega * (xn.y - q.y) + q.y;
+        xa.z = p.omega * (xn.z - q.z) + q.z;
+        xa.w = xn.w;
+        p.xnext[v] = xa;
+    }
+    if (KEEP_PP) p.pp[v] = xi;
+}
+
+// Inertial predictor (VBDsolver::forwardStep, VBD.cpp:103-112; TetMesh::applyGravity /
+// computeInertia / savePreviousPosition, TetMesh.h:319-348).  Free vertices are [0, nfree).
+__global__ void k_predict(const float4* __restrict__ x, float4* __restrict__ v, float4* __restrict__ xprev,
+                          float4* __restrict__ y, int nfree, int n, float h, float hgx, float hgy, float hgz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 xi = x[i];
+    xprev[i] = xi;
+    float4 yi = y[i];
+    if (i < nfree) {
+        float4 vi = v[i];
+        vi.x += hgx;
+        vi.y += hgy;
+        vi.z += hgz;
+        v[i] = vi;
+        yi.x = xi.x + h * vi.x;
+        yi.y = xi.y + h * vi.y;
+        yi.z = xi.z + h * vi.z;
+    } else {
+        yi.x = xi.x;
+        yi.y = xi.y;
+        yi.z = xi.z;
+    }
+    y[i] = yi;
+}
+
+// Velocity update v = (x - x_prev)/h * 0.999 (TetMesh::updateVelocity, TetMesh.h:305-311) and,
+// when the final positions sit in the second buffer, their copy back into the first.
+__global__ void k_finish(const float4* __restrict__ xf, float4* __restrict__ x0, const float4* __restrict__ xprev,
+                         float4* __restrict__ v, int nfree, float h, int copy_back, int update_v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfree) return;
+    const float4 xi = xf[i];
+    if (copy_back) x0[i] = xi;
+    if (update_v) {
+        const float4 xp = xprev[i];
+        float4 vi = v[i];
+        vi.x = ((xi.x - xp.x) / h) * 0.999f;
+        vi.y = ((xi.y - xp.y) / h) * 0.999f;
+        vi.z = ((xi.z - xp.z) / h) * 0.999f;
+        v[i] = vi;
+    }
+}
+
+// dst.xyz = src.xyz over [0, n), keeping dst.w (x = y start, VBD_GPU_Wrapper.cu:334).
+__global__ void k_copy_xyz(const float4* __restrict__ src, float4* __restrict__ d0, float4* __restrict__ d1, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 s = src[i];
+    float4 a = d0[i];
+    a.x = s.x; a.y = s.y; a.z = s.z;
+    d0[i] = a;
+    if (d1) {
+        float4 b = d1[i];
+        b.x = s.x; b.y = s.y; b.z = s.z;
+        d1[i] = b;
+    }
+}
+
+// Caller-order float[3N] <-> internal float4 (perm[i] = caller id of internal vertex i).
+__global__ void k_scatter3(const float* __restrict__ stage, const int* __restrict__ perm, float4* d0, float4* d1,
+                           int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int o = perm[i];
+    const float sx = stage[3 * o], sy = stage[3 * o + 1], sz = stage[3 * o + 2];
+    float4 a = d0[i];
+    a.x = sx; a.y = sy; a.z = sz;
+    d0[i] = a;
+    if (d1) {
+        float4 b = d1[i];
+        b.x = sx; b.y = sy; b.z = sz;
+        d1[i] = b;
+    }
+}
+
+__global__ void k_gather3(const float4* __restrict__ src, const int* __restrict__ perm, float* __restrict__ stage,
+                          int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int o = perm[i];
+    const float4 s = src[i];
+    stage[3 * o] = s.x;
+    stage[3 * o + 1] = s.y;
+    stage[3 * o + 2] = s.z;
+}
+
+// rec[t].c.zw = (mu, lambda); either array may be null.
+__global__ void k_set_materials(TetRec* rec, const float* __restrict__ mu, const float* __restrict__ lam, float mu0,
+                                float lam0, int ntet) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntet) return;
+    float4 c = rec[t].c;
+    c.z = mu ? mu[t] : (mu0 >= 0.f ? mu0 : c.z);
+    c.w = lam ? lam[t] : (lam0 >= 0.f ? lam0 : c.w);
+    rec[t].c = c;
+}
+
+// irec[j] = rec[inc_tet[j]]: the incidence-ordered copy.
+__global__ void k_pack_stream(const TetRec* __restrict__ rec, const int* __restrict__ inc_tet, TetRec* __restrict__ irec,
+                              int ninc) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ninc) return;
+    irec[j] = rec[inc_tet[j]];
+}
+
+// ---- FP64 reductions (energies, residual) ---------------------------------------------------
+
+template <int BS>
+__device__ __forceinline__ void block_sum_store(double val, double* partials) {
+    __shared__ double red[BS / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = val;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double w = threadIdx.x < BS / 32 ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if (threadIdx.x == 0) partials[blockIdx.x] = w;
+    }
+}
+
+// Sums partials[0..n) in a fixed order (deterministic) into out[0].
+__global__ void k_sum_partials(const double* __restrict__ partials, int n, double* __restrict__ out) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += partials[i];
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double w = threadIdx.x < (int)(blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if (threadIdx.x == 0) out[0] = w;
+    }
+}
+
+__device__ __forceinline__ void tet_F_double(const TetRec& r, const float4* __restrict__ X, double F[3][3]) {
+    const float4 p0 = X[r.ids.x], p1 = X[r.ids.y], p2 = X[r.ids.z], p3 = X[r.ids.w];
+    const double e[3][3] = {{(double)p1.x - p0.x, (double)p2.x - p0.x, (double)p3.x - p0.x},
+                            {(double)p1.y - p0.y, (double)p2.y - p0.y, (double)p3.y - p0.y},
+                            {(double)p1.z - p0.z, (double)p2.z - p0.z, (double)p3.z - p0.z}};
+    const double D[3][3] = {{r.a.x, r.a.y, r.a.z}, {r.a.w, r.b.x, r.b.y}, {r.b.z, r.b.w, r.c.x}};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) F[i][j] = e[i][0] * D[0][j] + e[i][1] * D[1][j] + e[i][2] * D[2][j];
+}
+
+__device__ __forceinline__ double det3d(const double F[3][3]) {
+    return F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) - F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+           F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+}
+
+// kind 0: incremental potential (inertia over vertices [0, nvert) + J-1 Neo-Hookean over tets)
+// kind 1: log-J Neo-Hookean elastic energy only (VBDsolver::computeTotalEnergy)
+__global__ void __launch_bounds__(256) k_energy(const float4* __restrict__ X, const float4* __restrict__ Y,
+                                                const TetRec* __restrict__ rec, int nvert, int ntet, int kind,
+                                                double inv_h2, double* __restrict__ partials) {
+    double acc = 0.0;
+    const int stride = gridDim.x * blockDim.x;
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (kind == 0) {
+        for (int i = t0; i < nvert; i += stride) {
+            const float4 x = X[i], y = Y[i];
+            const double dx = (double)x.x - y.x, dy = (double)x.y - y.y, dz = (double)x.z - y.z;
+            acc += 0.5 * (double)y.w * inv_h2 * (dx * dx + dy * dy + dz * dz);
+        }
+    }
+    for (int t = t0; t < ntet; t += stride) {
+        const TetRec r = load_rec(rec + t);
+        double F[3][3];
+        tet_F_double(r, X, F);
+        double tr = 0.0;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) tr += F[i][j] * F[i][j];
+        const double J = det3d(F);
+        const double mu = r.c.z, lam = r.c.w, V0 = r.c.y;
+        double psi;
+        if (kind == 0) {
+            psi = 0.5 * mu * (tr - 3.0) - mu * (J - 1.0) + 0.5 * lam * (J - 1.0) * (J - 1.0);
+        } else {
+            const double lj = log(fabs(J));
+            psi = 0.5 * mu * (tr - 3.0) - mu * lj + 0.5 * lam * lj * lj;
+        }
+        acc += V0 * psi;
+    }
+    block_sum_store<256>(acc, partials);
+}
+
+// |m/h^2 (x - y) + dE/dx|^2 summed over the free vertices [v_begin, v_end): one LANES-thread
+// group per vertex as in k_sweep, one FP64 partial per block.
+template <int LANES>
+__global__ void __launch_bounds__(256) k_residual(SweepParams p, double* __restrict__ partials) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & (LANES - 1);
+    const int v = p.v_begin + t / LANES;
+    const bool active = v < p.v_end;
+    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
+    int j0 = 0, j1 = 0;
+    if (active) {
+        xi = p.x[v];
+        j0 = p.inc_off[v];
+        j1 = p.inc_off[v + 1];
+    }
+    Acc a;
+    a.zero();
+    for (int j = j0 + lane; j < j1; j += LANES) {
+        const TetRec r = load_rec(p.rec + p.inc_tet[j]);
+        tet_contrib<false>(r, v, xi, p.x, a);
+    }
+    group_reduce<LANES>(a);
+    double r2 = 0.0;
+    if (active && lane == 0) {
+        const float4 yi = p.y[v];
+        const double cm = (double)yi.w * p.dtsr;
+        const double r0 = cm * ((double)xi.x - yi.x) + a.g0;
+        const double r1 = cm * ((double)xi.y - yi.y) + a.g1;
+        const double rz = cm * ((double)xi.z - yi.z) + a.g2;
+        r2 = r0 * r0 + r1 * r1 + rz * rz;
+    }
+    block_sum_store<256>(r2, partials);
+}
+
+}  // namespace vbd

@@ -1,0 +1,815 @@
+// Solver handle of libvbd_b200: device state, launch sequencing, CUDA-graph replay and the
+// solver half of the C ABI declared in include/vbd_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "vbd_b200.h"
+#include "vbd_internal.h"
+#include "vbd_kernels.cuh"
+
+namespace vbd {
+
+#define CUDA_TRY(call)                                                                                 \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            VBD_FAIL(VBD_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+#define VBD_TRY(expr)            \
+    do {                         \
+        int rc_ = (expr);        \
+        if (rc_) return rc_;     \
+    } while (0)
+
+template <class T> struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    int alloc(size_t count) {
+        release();
+        if (count == 0) return VBD_OK;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            VBD_FAIL(VBD_ERR_ALLOC, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+        }
+        n = count;
+        return VBD_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DBuf() { release(); }
+};
+
+static inline unsigned nblk(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// getAcceleratorOmega (VBD.cpp:302-311): double literals, float result.
+static float omega_of(int order, float rho, float prev) {
+    if (order == 1) return 1.0f;
+    if (order == 2) return (float)(2.0 / (2.0 - (double)(rho * rho)));
+    return (float)(4.0 / (4.0 - (double)(rho * rho * prev)));
+}
+
+using SweepFn = void (*)(SweepParams);
+
+template <int L, bool S, bool A, bool K> static SweepFn sweep_fn() { return &k_sweep<L, S, A, K>; }
+
+template <int L> static SweepFn pick_sweep(bool stream, bool accel, bool keep) {
+    if (stream) {
+        if (accel) return keep ? sweep_fn<L, true, true, true>() : sweep_fn<L, true, true, false>();
+        return keep ? sweep_fn<L, true, false, true>() : sweep_fn<L, true, false, false>();
+    }
+    if (accel) return keep ? sweep_fn<L, false, true, true>() : sweep_fn<L, false, true, false>();
+    return keep ? sweep_fn<L, false, false, true>() : sweep_fn<L, false, false, false>();
+}
+
+static SweepFn pick_sweep(int lanes, bool stream, bool accel, bool keep) {
+    switch (lanes) {
+        case 4: return pick_sweep<4>(stream, accel, keep);
+        case 8: return pick_sweep<8>(stream, accel, keep);
+        case 16: return pick_sweep<16>(stream, accel, keep);
+        default: return pick_sweep<32>(stream, accel, keep);
+    }
+}
+
+// Key of a captured step / solve graph: everything baked into its kernel parameters.
+struct GraphKey {
+    int kind;  // 0 = step, 1 = solve, 2 = single sweep
+    int iters, accel, init, lanes, layout;
+    float h, dtsr, hg[3], rho;
+    bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
+};
+
+struct GraphEntry {
+    GraphKey key;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    size_t nodes = 0;
+};
+
+}  // namespace vbd
+
+struct vbd_solver {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int N = 0, T = 0, C = 0, nfree = 0;
+    long long ninc = 0;
+    bool ready = false, have_materials = false;
+    std::vector<int> cstart;  // colour c = internal ids [cstart[c], cstart[c+1])
+    vbd::DBuf<float4> x0, x1, pp, y, v, xprev;
+    vbd::DBuf<int> perm, inc_off, inc_tet;
+    vbd::DBuf<vbd::TetRec> rec, irec;
+    vbd::DBuf<float> stage, mat_stage;
+    vbd::DBuf<unsigned long long> status;
+    vbd::DBuf<double> partials, scalar;
+    int lanes = 8, layout = 0, use_graph = 1, timing = 0;
+    long long launches = 0;
+    std::vector<vbd::GraphEntry> graphs;
+    std::vector<double> colour_bytes;               // algorithmic bytes of one sweep of colour c
+    std::vector<cudaEvent_t> ev_pool;               // event pairs of timed sweeps
+    std::vector<double> ev_bytes;                   // bytes of each timed sweep
+    size_t ev_used = 0;                             // pairs in use
+    double timed_ms = 0.0, timed_bytes = 0.0;
+    long long timed_launches = 0;
+
+    ~vbd_solver() {
+        drop_graphs();
+        for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+
+    // Folds the recorded event pairs into the running totals (synchronises on the last one).
+    int collect_timing() {
+        if (ev_used == 0) return VBD_OK;
+        CUDA_TRY(cudaEventSynchronize(ev_pool[2 * ev_used - 1]));
+        for (size_t k = 0; k < ev_used; ++k) {
+            float ms = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&ms, ev_pool[2 * k], ev_pool[2 * k + 1]));
+            timed_ms += ms;
+            timed_bytes += ev_bytes[k];
+        }
+        timed_launches += (long long)ev_used;
+        ev_used = 0;
+        ev_bytes.clear();
+        return VBD_OK;
+    }
+
+    int timing_event(cudaEvent_t* out) {
+        if (ev_pool.size() < 2 * (ev_used + 1)) {
+            if (ev_used >= 4096) VBD_TRY(collect_timing());
+            while (ev_pool.size() < 2 * (ev_used + 1)) {
+                cudaEvent_t e;
+                CUDA_TRY(cudaEventCreate(&e));
+                ev_pool.push_back(e);
+            }
+        }
+        out[0] = ev_pool[2 * ev_used];
+        out[1] = ev_pool[2 * ev_used + 1];
+        return VBD_OK;
+    }
+
+    void drop_graphs() {
+        for (auto& g : graphs) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            if (g.graph) cudaGraphDestroy(g.graph);
+        }
+        graphs.clear();
+    }
+
+    int check_launch() {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) VBD_FAIL(VBD_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+        ++launches;
+        return VBD_OK;
+    }
+
+    int launch_sweep(int c, float4* xr, float4* xn, bool accel, bool keep_pp, float dtsr, float omega) {
+        const int vb = cstart[c], ve = cstart[c + 1];
+        if (ve <= vb) return VBD_OK;
+        vbd::SweepParams p{xr,        xn,    pp.p,        y.p,  inc_off.p, inc_tet.p, rec.p,
+                           irec.p,    status.p, vb,       ve,   dtsr,      omega};
+        const long long threads = (long long)(ve - vb) * lanes;
+        vbd::SweepFn fn = vbd::pick_sweep(lanes, layout == 1, accel, keep_pp);
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        if (timing) {
+            VBD_TRY(timing_event(ev));
+            CUDA_TRY(cudaEventRecord(ev[0], stream));
+        }
+        fn<<<vbd::nblk(threads, 256), 256, 0, stream>>>(p);
+        VBD_TRY(check_launch());
+        if (timing) {
+            CUDA_TRY(cudaEventRecord(ev[1], stream));
+            ev_bytes.push_back(colour_bytes[c]);
+            ++ev_used;
+        }
+        return VBD_OK;
+    }
+
+    // `iters` sweeps with the Chebyshev schedule; `cur` tracks which buffer holds x.
+    int emit_iterations(int iters, float dtsr, bool accel, float rho, int& cur) {
+        float omega = 1.0f;
+        for (int k = 1; k <= iters; ++k) {
+            bool blend = false;
+            if (accel) {
+                omega = vbd::omega_of(k, rho, omega);
+                blend = omega > 1.0f;
+            }
+            float4* xr = cur ? x1.p : x0.p;
+            float4* xo = cur ? x0.p : x1.p;
+            for (int c = 0; c < C; ++c) VBD_TRY(launch_sweep(c, xr, xo, blend, accel, dtsr, omega));
+            if (blend) cur ^= 1;
+        }
+        return VBD_OK;
+    }
+
+    int emit_substep(float h, float dtsr, const float* hg, int iters, bool accel, float rho) {
+        vbd::k_predict<<<vbd::nblk(N, 256), 256, 0, stream>>>(x0.p, v.p, xprev.p, y.p, nfree, N, h, hg[0], hg[1],
+                                                              hg[2]);
+        VBD_TRY(check_launch());
+        int cur = 0;
+        VBD_TRY(emit_iterations(iters, dtsr, accel, rho, cur));
+        if (nfree > 0) {
+            vbd::k_finish<<<vbd::nblk(nfree, 256), 256, 0, stream>>>(cur ? x1.p : x0.p, x0.p, xprev.p, v.p, nfree, h,
+                                                                     cur, 1);
+            VBD_TRY(check_launch());
+        }
+        return VBD_OK;
+    }
+
+    int emit_solve(int iters, float dtsr, bool accel, float rho, int init) {
+        if (init == VBD_INIT_FROM_INERTIA) {
+            vbd::k_copy_xyz<<<vbd::nblk(N, 256), 256, 0, stream>>>(y.p, x0.p, x1.p, N);
+            VBD_TRY(check_launch());
+        }
+        int cur = 0;
+        VBD_TRY(emit_iterations(iters, dtsr, accel, rho, cur));
+        if (cur && nfree > 0) {
+            vbd::k_finish<<<vbd::nblk(nfree, 256), 256, 0, stream>>>(x1.p, x0.p, nullptr, nullptr, nfree, 1.0f, 1, 0);
+            VBD_TRY(check_launch());
+        }
+        return VBD_OK;
+    }
+
+    template <class Emit> int run(const vbd::GraphKey& key, Emit emit) {
+        if (!use_graph || timing) return emit();
+        vbd::GraphEntry* hit = nullptr;
+        for (auto& g : graphs)
+            if (g.key == key) hit = &g;
+        if (!hit) {
+            vbd::GraphEntry e;
+            e.key = key;
+            const long long saved = launches;
+            CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            int rc = emit();
+            cudaGraph_t g = nullptr;
+            cudaError_t ce = cudaStreamEndCapture(stream, &g);
+            launches = saved;
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (ce != cudaSuccess) VBD_FAIL(VBD_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+            e.graph = g;
+            CUDA_TRY(cudaGraphGetNodes(g, nullptr, &e.nodes));
+            cudaError_t ie = cudaGraphInstantiate(&e.exec, g, 0);
+            if (ie != cudaSuccess) {
+                cudaGraphDestroy(g);
+                VBD_FAIL(VBD_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ie));
+            }
+            if (graphs.size() >= 16) {
+                cudaGraphExecDestroy(graphs.front().exec);
+                cudaGraphDestroy(graphs.front().graph);
+                graphs.erase(graphs.begin());
+            }
+            graphs.push_back(e);
+            hit = &graphs.back();
+        }
+        CUDA_TRY(cudaGraphLaunch(hit->exec, stream));
+        launches += (long long)hit->nodes;
+        return VBD_OK;
+    }
+
+    int upload3(const float* src, float4* d0, float4* d1) {
+        CUDA_TRY(cudaMemcpyAsync(stage.p, src, sizeof(float) * 3 * (size_t)N, cudaMemcpyDefault, stream));
+        vbd::k_scatter3<<<vbd::nblk(N, 256), 256, 0, stream>>>(stage.p, perm.p, d0, d1, N);
+        VBD_TRY(check_launch());
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        return VBD_OK;
+    }
+
+    int download3(const float4* src, float* dst) {
+        vbd::k_gather3<<<vbd::nblk(N, 256), 256, 0, stream>>>(src, perm.p, stage.p, N);
+        VBD_TRY(check_launch());
+        CUDA_TRY(cudaMemcpyAsync(dst, stage.p, sizeof(float) * 3 * (size_t)N, cudaMemcpyDefault, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        return VBD_OK;
+    }
+
+    int repack_stream() {
+        if (layout != 1) {
+            irec.release();
+            return VBD_OK;
+        }
+        if (irec.n != (size_t)ninc) VBD_TRY(irec.alloc(ninc));
+        if (ninc > 0) {
+            vbd::k_pack_stream<<<vbd::nblk(ninc, 256), 256, 0, stream>>>(rec.p, inc_tet.p, irec.p, (int)ninc);
+            VBD_TRY(check_launch());
+        }
+        return VBD_OK;
+    }
+
+    int reduce_scalar(unsigned blocks, double* out) {
+        vbd::k_sum_partials<<<1, 1024, 0, stream>>>(partials.p, (int)blocks, scalar.p);
+        VBD_TRY(check_launch());
+        CUDA_TRY(cudaMemcpyAsync(out, scalar.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        return VBD_OK;
+    }
+};
+
+namespace {
+
+struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(int d) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+int need_ready(vbd_solver* s) {
+    if (!s) VBD_FAIL(VBD_ERR_INVALID_ARG, "null solver handle");
+    if (!s->ready) VBD_FAIL(VBD_ERR_STATE, "solver has no mesh: call vbd_solver_init first");
+    return VBD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vbd_solver_create(vbd_solver** out, int device, void* cuda_stream) {
+    vbd::clear_error();
+    if (!out) VBD_FAIL(VBD_ERR_INVALID_ARG, "out is null");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        VBD_FAIL(VBD_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= count) VBD_FAIL(VBD_ERR_NO_DEVICE, "device %d out of range (%d devices)", device, count);
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10 || prop.minor != 0)
+        VBD_FAIL(VBD_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a only", device,
+                 prop.major, prop.minor);
+    DeviceScope scope(device);
+    std::unique_ptr<vbd_solver> s(new vbd_solver());
+    s->device = device;
+    if (cuda_stream) {
+        s->stream = static_cast<cudaStream_t>(cuda_stream);
+    } else {
+        CUDA_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+        s->own_stream = true;
+    }
+    VBD_TRY(s->status.alloc(vbd::ST_SLOTS));
+    CUDA_TRY(cudaMemset(s->status.p, 0, sizeof(unsigned long long) * vbd::ST_SLOTS));
+    VBD_TRY(s->scalar.alloc(1));
+    *out = s.release();
+    return VBD_OK;
+}
+
+int vbd_solver_destroy(vbd_solver* s) {
+    vbd::clear_error();
+    if (!s) return VBD_OK;
+    DeviceScope scope(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    delete s;
+    return VBD_OK;
+}
+
+int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions, const float* velocities,
+                    const float* inertia, const float* vertex_mass, const uint8_t* fixed, const int32_t* tets,
+                    int32_t num_colours, const int32_t* group_offsets, const int32_t* group_vertices,
+                    const float* dm_inv, const float* rest_vol, const float* tet_mu, const float* tet_lambda) {
+    vbd::clear_error();
+    if (!s) VBD_FAIL(VBD_ERR_INVALID_ARG, "null solver handle");
+    if (N <= 0) VBD_FAIL(VBD_ERR_INVALID_ARG, "num_verts must be positive (got %d)", N);
+    if (T < 0) VBD_FAIL(VBD_ERR_INVALID_ARG, "num_tets is negative");
+    if (!positions || !vertex_mass || !fixed) VBD_FAIL(VBD_ERR_INVALID_ARG, "positions, vertex_mass, fixed are required");
+    if (T > 0 && (!dm_inv || !rest_vol)) VBD_FAIL(VBD_ERR_INVALID_ARG, "dm_inv and rest_vol are required");
+    if (num_colours < 0 || (num_colours > 0 && (!group_offsets || !group_vertices)))
+        VBD_FAIL(VBD_ERR_INVALID_ARG, "colour groups missing");
+    if ((tet_mu == nullptr) != (tet_lambda == nullptr))
+        VBD_FAIL(VBD_ERR_INVALID_ARG, "give both tet_mu and tet_lambda, or neither");
+    if ((long long)T * 4 > 0x7fffffffLL) VBD_FAIL(VBD_ERR_INVALID_ARG, "too many tets for 32-bit incidence ids");
+    VBD_TRY(vbd::check_tets(N, T, tets));
+    // colour groups: a partition of the vertices into independent sets
+    if (num_colours == 0 || group_offsets[0] != 0 || group_offsets[num_colours] != N)
+        VBD_FAIL(VBD_ERR_INVALID_ARG, "colour groups must cover all %d vertices", N);
+    std::vector<int32_t> colour(N, -1);
+    for (int c = 0; c < num_colours; ++c) {
+        if (group_offsets[c + 1] < group_offsets[c]) VBD_FAIL(VBD_ERR_INVALID_ARG, "colour offsets decrease at %d", c);
+        for (int k = group_offsets[c]; k < group_offsets[c + 1]; ++k) {
+            int vtx = group_vertices[k];
+            if (vtx < 0 || vtx >= N) VBD_FAIL(VBD_ERR_INVALID_ARG, "colour group %d holds vertex %d out of range", c, vtx);
+            if (colour[vtx] != -1) VBD_FAIL(VBD_ERR_INVALID_ARG, "vertex %d appears in two colour groups", vtx);
+            colour[vtx] = c;
+        }
+    }
+    for (int t = 0; t < T; ++t) {
+        const int32_t* q = tets + 4LL * t;
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < a; ++b)
+                if (colour[q[a]] == colour[q[b]])
+                    VBD_FAIL(VBD_ERR_INVALID_ARG,
+                             "colour groups are not independent: vertices %d and %d of tet %d share colour %d", q[a],
+                             q[b], t, colour[q[a]]);
+    }
+    for (int i = 0; i < N; ++i)
+        if (!(vertex_mass[i] >= 0.0f) || !std::isfinite(vertex_mass[i]))
+            VBD_FAIL(VBD_ERR_INVALID_ARG, "vertex_mass[%d] is negative or not finite", i);
+
+    DeviceScope scope(s->device);
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->ready = false;
+    s->drop_graphs();
+
+    // Internal order: free vertices colour by colour (group order), then the pinned ones.
+    std::vector<int32_t> perm;
+    perm.reserve(N);
+    std::vector<int> cstart(num_colours + 1, 0);
+    for (int c = 0; c < num_colours; ++c) {
+        cstart[c] = (int)perm.size();
+        for (int k = group_offsets[c]; k < group_offsets[c + 1]; ++k)
+            if (!fixed[group_vertices[k]]) perm.push_back(group_vertices[k]);
+    }
+    cstart[num_colours] = (int)perm.size();
+    const int nfree = (int)perm.size();
+    for (int i = 0; i < N; ++i)
+        if (fixed[i]) perm.push_back(i);
+    std::vector<int32_t> iperm(N);
+    for (int i = 0; i < N; ++i) iperm[perm[i]] = i;
+
+    // Incident tets of each free vertex, ascending tet id (TetMesh::vertAdjacentTets).
+    std::vector<int32_t> voff(N + 1), vtets(4LL * T);
+    vbd::build_vertex_tets(N, T, tets, voff.data(), vtets.data());
+    std::vector<int32_t> inc_off(N + 1, 0);
+    for (int i = 0; i < nfree; ++i) inc_off[i + 1] = inc_off[i] + (voff[perm[i] + 1] - voff[perm[i]]);
+    for (int i = nfree; i < N; ++i) inc_off[i + 1] = inc_off[i];
+    const long long ninc = inc_off[N];
+    std::vector<int32_t> inc_tet(std::max<long long>(ninc, 1));
+    for (int i = 0; i < nfree; ++i)
+        std::copy(vtets.begin() + voff[perm[i]], vtets.begin() + voff[perm[i] + 1], inc_tet.begin() + inc_off[i]);
+
+    std::vector<vbd::TetRec> rec(std::max(T, 1));
+    for (int t = 0; t < T; ++t) {
+        const int32_t* q = tets + 4LL * t;
+        const float* d = dm_inv + 9LL * t;
+        vbd::TetRec& r = rec[t];
+        r.ids = make_int4(iperm[q[0]], iperm[q[1]], iperm[q[2]], iperm[q[3]]);
+        r.a = make_float4(d[0], d[1], d[2], d[3]);
+        r.b = make_float4(d[4], d[5], d[6], d[7]);
+        r.c = make_float4(d[8], rest_vol[t], tet_mu ? tet_mu[t] : 0.0f, tet_lambda ? tet_lambda[t] : 0.0f);
+    }
+
+    std::vector<float4> hx(N), hv(N), hy(N);
+    for (int i = 0; i < N; ++i) {
+        const int o = perm[i];
+        hx[i] = make_float4(positions[3LL * o], positions[3LL * o + 1], positions[3LL * o + 2], 0.0f);
+        hv[i] = velocities ? make_float4(velocities[3LL * o], velocities[3LL * o + 1], velocities[3LL * o + 2], 0.0f)
+                           : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float* yy = inertia ? inertia + 3LL * o : positions + 3LL * o;
+        hy[i] = make_float4(yy[0], yy[1], yy[2], vertex_mass[o]);
+    }
+
+    VBD_TRY(s->x0.alloc(N));
+    VBD_TRY(s->x1.alloc(N));
+    VBD_TRY(s->pp.alloc(N));
+    VBD_TRY(s->y.alloc(N));
+    VBD_TRY(s->v.alloc(N));
+    VBD_TRY(s->xprev.alloc(N));
+    VBD_TRY(s->perm.alloc(N));
+    VBD_TRY(s->inc_off.alloc(N + 1));
+    VBD_TRY(s->inc_tet.alloc(inc_tet.size()));
+    VBD_TRY(s->rec.alloc(rec.size()));
+    VBD_TRY(s->stage.alloc(3LL * N));
+    VBD_TRY(s->mat_stage.alloc(2LL * std::max(T, 1)));
+    const long long max_blocks = std::max<long long>(4096, vbd::nblk((long long)N * 32, 256));
+    VBD_TRY(s->partials.alloc(max_blocks));
+    const size_t b4 = sizeof(float4) * (size_t)N;
+    CUDA_TRY(cudaMemcpy(s->x0.p, hx.data(), b4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->x1.p, hx.data(), b4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->xprev.p, hx.data(), b4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->pp.p, hx.data(), b4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->v.p, hv.data(), b4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->y.p, hy.data(), b4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->perm.p, perm.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->inc_off.p, inc_off.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->inc_tet.p, inc_tet.data(), sizeof(int) * inc_tet.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->rec.p, rec.data(), sizeof(vbd::TetRec) * rec.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemset(s->status.p, 0, sizeof(unsigned long long) * vbd::ST_SLOTS));
+
+    s->colour_bytes.assign(num_colours, 0.0);
+    for (int c = 0; c < num_colours; ++c)
+        for (int i = cstart[c]; i < cstart[c + 1]; ++i)
+            s->colour_bytes[c] += 60.0 * (inc_off[i + 1] - inc_off[i]) + 96.0;
+    s->N = N;
+    s->T = T;
+    s->C = num_colours;
+    s->nfree = nfree;
+    s->ninc = ninc;
+    s->cstart = cstart;
+    s->have_materials = tet_mu != nullptr;
+    VBD_TRY(s->repack_stream());
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->ready = true;
+    return VBD_OK;
+}
+
+int vbd_solver_set_materials(vbd_solver* s, const float* tet_mu, const float* tet_lambda) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!tet_mu && !tet_lambda) return VBD_OK;
+    if (!s->have_materials && !(tet_mu && tet_lambda))
+        VBD_FAIL(VBD_ERR_STATE, "materials were never set: give both tet_mu and tet_lambda");
+    DeviceScope scope(s->device);
+    if (s->T == 0) {
+        s->have_materials = true;
+        return VBD_OK;
+    }
+    float* dmu = nullptr;
+    float* dlam = nullptr;
+    if (tet_mu) {
+        dmu = s->mat_stage.p;
+        CUDA_TRY(cudaMemcpyAsync(dmu, tet_mu, sizeof(float) * s->T, cudaMemcpyDefault, s->stream));
+    }
+    if (tet_lambda) {
+        dlam = s->mat_stage.p + s->T;
+        CUDA_TRY(cudaMemcpyAsync(dlam, tet_lambda, sizeof(float) * s->T, cudaMemcpyDefault, s->stream));
+    }
+    vbd::k_set_materials<<<vbd::nblk(s->T, 256), 256, 0, s->stream>>>(s->rec.p, dmu, dlam, -1.f, -1.f, s->T);
+    VBD_TRY(s->check_launch());
+    VBD_TRY(s->repack_stream());
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->have_materials = true;
+    return VBD_OK;
+}
+
+int vbd_solver_set_uniform_material(vbd_solver* s, float mu, float lambda) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!(mu >= 0.f) || !(lambda >= 0.f) || !std::isfinite(mu) || !std::isfinite(lambda))
+        VBD_FAIL(VBD_ERR_INVALID_ARG, "mu and lambda must be finite and non-negative");
+    DeviceScope scope(s->device);
+    if (s->T > 0) {
+        vbd::k_set_materials<<<vbd::nblk(s->T, 256), 256, 0, s->stream>>>(s->rec.p, nullptr, nullptr, mu, lambda,
+                                                                          s->T);
+        VBD_TRY(s->check_launch());
+        VBD_TRY(s->repack_stream());
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+    }
+    s->have_materials = true;
+    return VBD_OK;
+}
+
+int vbd_solver_set_positions(vbd_solver* s, const float* xyz) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!xyz) VBD_FAIL(VBD_ERR_INVALID_ARG, "xyz is null");
+    DeviceScope scope(s->device);
+    return s->upload3(xyz, s->x0.p, s->x1.p);
+}
+
+int vbd_solver_get_positions(vbd_solver* s, float* xyz) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!xyz) VBD_FAIL(VBD_ERR_INVALID_ARG, "xyz is null");
+    DeviceScope scope(s->device);
+    return s->download3(s->x0.p, xyz);
+}
+
+int vbd_solver_set_velocities(vbd_solver* s, const float* xyz) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!xyz) VBD_FAIL(VBD_ERR_INVALID_ARG, "xyz is null");
+    DeviceScope scope(s->device);
+    return s->upload3(xyz, s->v.p, nullptr);
+}
+
+int vbd_solver_get_velocities(vbd_solver* s, float* xyz) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!xyz) VBD_FAIL(VBD_ERR_INVALID_ARG, "xyz is null");
+    DeviceScope scope(s->device);
+    return s->download3(s->v.p, xyz);
+}
+
+int vbd_solver_set_inertia(vbd_solver* s, const float* xyz) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!xyz) VBD_FAIL(VBD_ERR_INVALID_ARG, "xyz is null");
+    DeviceScope scope(s->device);
+    return s->upload3(xyz, s->y.p, nullptr);
+}
+
+int vbd_solver_get_inertia(vbd_solver* s, float* xyz) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!xyz) VBD_FAIL(VBD_ERR_INVALID_ARG, "xyz is null");
+    DeviceScope scope(s->device);
+    return s->download3(s->y.p, xyz);
+}
+
+int vbd_solver_solve(vbd_solver* s, int32_t iterations, float dt_sqr_reciprocal, int32_t use_acceleration, float rho,
+                     int32_t init_mode) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!s->have_materials) VBD_FAIL(VBD_ERR_STATE, "materials not set");
+    if (iterations < 0) VBD_FAIL(VBD_ERR_INVALID_ARG, "iterations must be >= 0");
+    if (!(dt_sqr_reciprocal > 0.f) || !std::isfinite(dt_sqr_reciprocal))
+        VBD_FAIL(VBD_ERR_INVALID_ARG, "dt_sqr_reciprocal must be positive and finite");
+    if (init_mode != VBD_INIT_FROM_POSITIONS && init_mode != VBD_INIT_FROM_INERTIA)
+        VBD_FAIL(VBD_ERR_INVALID_ARG, "unknown init_mode %d", init_mode);
+    DeviceScope scope(s->device);
+    vbd::GraphKey key{};
+    key.kind = 1;
+    key.iters = iterations;
+    key.accel = use_acceleration ? 1 : 0;
+    key.init = init_mode;
+    key.lanes = s->lanes;
+    key.layout = s->layout;
+    key.dtsr = dt_sqr_reciprocal;
+    key.rho = rho;
+    return s->run(key, [&] { return s->emit_solve(iterations, dt_sqr_reciprocal, use_acceleration != 0, rho, init_mode); });
+}
+
+int vbd_solver_solve_iteration(vbd_solver* s, float dt_sqr_reciprocal) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!s->have_materials) VBD_FAIL(VBD_ERR_STATE, "materials not set");
+    if (!(dt_sqr_reciprocal > 0.f) || !std::isfinite(dt_sqr_reciprocal))
+        VBD_FAIL(VBD_ERR_INVALID_ARG, "dt_sqr_reciprocal must be positive and finite");
+    DeviceScope scope(s->device);
+    int cur = 0;
+    return s->emit_iterations(1, dt_sqr_reciprocal, false, 0.f, cur);
+}
+
+int vbd_solver_step(vbd_solver* s, float dt, int32_t substeps, int32_t iterations, const float* gravity,
+                    int32_t use_acceleration, float rho) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!s->have_materials) VBD_FAIL(VBD_ERR_STATE, "materials not set");
+    if (!(dt > 0.f) || !std::isfinite(dt)) VBD_FAIL(VBD_ERR_INVALID_ARG, "dt must be positive and finite");
+    if (substeps < 1) VBD_FAIL(VBD_ERR_INVALID_ARG, "substeps must be >= 1");
+    if (iterations < 0) VBD_FAIL(VBD_ERR_INVALID_ARG, "iterations must be >= 0");
+    if (!gravity) VBD_FAIL(VBD_ERR_INVALID_ARG, "gravity is null");
+    DeviceScope scope(s->device);
+    const float h = dt / (float)substeps;
+    const float dtsr = (float)(1.0 / (double)(h * h));
+    const float hg[3] = {h * gravity[0], h * gravity[1], h * gravity[2]};
+    vbd::GraphKey key{};
+    key.kind = 0;
+    key.iters = iterations;
+    key.accel = use_acceleration ? 1 : 0;
+    key.lanes = s->lanes;
+    key.layout = s->layout;
+    key.h = h;
+    key.dtsr = dtsr;
+    key.hg[0] = hg[0];
+    key.hg[1] = hg[1];
+    key.hg[2] = hg[2];
+    key.rho = rho;
+    for (int k = 0; k < substeps; ++k)
+        VBD_TRY(s->run(key, [&] { return s->emit_substep(h, dtsr, hg, iterations, use_acceleration != 0, rho); }));
+    return VBD_OK;
+}
+
+int vbd_solver_sync(vbd_solver* s) {
+    vbd::clear_error();
+    if (!s) VBD_FAIL(VBD_ERR_INVALID_ARG, "null solver handle");
+    DeviceScope scope(s->device);
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return VBD_OK;
+}
+
+int vbd_solver_energy(vbd_solver* s, int32_t kind, float h, double* out) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!out) VBD_FAIL(VBD_ERR_INVALID_ARG, "out is null");
+    if (kind < 0 || kind > 2) VBD_FAIL(VBD_ERR_INVALID_ARG, "unknown energy kind %d", kind);
+    if (kind != VBD_ENERGY_ELASTIC_LOGJ && (!(h > 0.f) || !std::isfinite(h)))
+        VBD_FAIL(VBD_ERR_INVALID_ARG, "h must be positive and finite");
+    DeviceScope scope(s->device);
+    if (kind == VBD_ENERGY_RESIDUAL) {
+        if (s->nfree == 0) {
+            *out = 0.0;
+            return VBD_OK;
+        }
+        vbd::SweepParams p{s->x0.p, nullptr, s->pp.p, s->y.p, s->inc_off.p, s->inc_tet.p, s->rec.p, s->irec.p,
+                           s->status.p, 0, s->nfree, (float)(1.0 / ((double)h * h)), 1.0f};
+        const int L = s->lanes;
+        const unsigned blocks = vbd::nblk((long long)s->nfree * L, 256);
+        switch (L) {
+            case 4: vbd::k_residual<4><<<blocks, 256, 0, s->stream>>>(p, s->partials.p); break;
+            case 8: vbd::k_residual<8><<<blocks, 256, 0, s->stream>>>(p, s->partials.p); break;
+            case 16: vbd::k_residual<16><<<blocks, 256, 0, s->stream>>>(p, s->partials.p); break;
+            default: vbd::k_residual<32><<<blocks, 256, 0, s->stream>>>(p, s->partials.p); break;
+        }
+        VBD_TRY(s->check_launch());
+        double r2 = 0.0;
+        VBD_TRY(s->reduce_scalar(blocks, &r2));
+        *out = std::sqrt(r2);
+        return VBD_OK;
+    }
+    const long long work = std::max<long long>(kind == VBD_ENERGY_IP ? s->N : 0, s->T);
+    const unsigned blocks = std::max(1u, std::min<unsigned>(vbd::nblk(work, 256), 4096u));
+    const double inv_h2 = kind == VBD_ENERGY_IP ? 1.0 / ((double)h * h) : 0.0;
+    vbd::k_energy<<<blocks, 256, 0, s->stream>>>(s->x0.p, s->y.p, s->rec.p, kind == VBD_ENERGY_IP ? s->N : 0, s->T,
+                                                 kind, inv_h2, s->partials.p);
+    VBD_TRY(s->check_launch());
+    return s->reduce_scalar(blocks, out);
+}
+
+int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite, int32_t reset) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    DeviceScope scope(s->device);
+    unsigned long long h[vbd::ST_SLOTS];
+    CUDA_TRY(cudaMemcpyAsync(h, s->status.p, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (singular_skips) *singular_skips = (int64_t)h[vbd::ST_SINGULAR];
+    if (nonfinite) *nonfinite = h[vbd::ST_NONFINITE] ? 1 : 0;
+    if (reset) {
+        CUDA_TRY(cudaMemsetAsync(s->status.p, 0, sizeof(h), s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+    }
+    return VBD_OK;
+}
+
+int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
+    vbd::clear_error();
+    if (!s) VBD_FAIL(VBD_ERR_INVALID_ARG, "null solver handle");
+    DeviceScope scope(s->device);
+    switch (option) {
+        case VBD_OPT_LANES:
+            if (value != 4 && value != 8 && value != 16 && value != 32)
+                VBD_FAIL(VBD_ERR_INVALID_ARG, "lanes must be 4, 8, 16 or 32");
+            s->lanes = value;
+            return VBD_OK;
+        case VBD_OPT_LAYOUT:
+            if (value != 0 && value != 1) VBD_FAIL(VBD_ERR_INVALID_ARG, "layout must be 0 or 1");
+            s->layout = value;
+            if (s->ready) {
+                VBD_TRY(s->repack_stream());
+                CUDA_TRY(cudaStreamSynchronize(s->stream));
+            }
+            return VBD_OK;
+        case VBD_OPT_GRAPH:
+            s->use_graph = value ? 1 : 0;
+            return VBD_OK;
+        case VBD_OPT_KERNEL_TIMING:
+            s->timing = value ? 1 : 0;
+            return VBD_OK;
+        default:
+            VBD_FAIL(VBD_ERR_INVALID_ARG, "unknown option %d", option);
+    }
+}
+
+int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value) {
+    vbd::clear_error();
+    if (!s || !value) VBD_FAIL(VBD_ERR_INVALID_ARG, "null argument");
+    switch (option) {
+        case VBD_OPT_LANES: *value = s->lanes; return VBD_OK;
+        case VBD_OPT_LAYOUT: *value = s->layout; return VBD_OK;
+        case VBD_OPT_GRAPH: *value = s->use_graph; return VBD_OK;
+        case VBD_OPT_KERNEL_TIMING: *value = s->timing; return VBD_OK;
+        default: VBD_FAIL(VBD_ERR_INVALID_ARG, "unknown option %d", option);
+    }
+}
+
+int vbd_solver_info(vbd_solver* s, int32_t* num_verts, int32_t* num_tets, int32_t* num_colours) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (num_verts) *num_verts = s->N;
+    if (num_tets) *num_tets = s->T;
+    if (num_colours) *num_colours = s->C;
+    return VBD_OK;
+}
+
+int vbd_solver_kernel_time(vbd_solver* s, double* sweep_ms, int64_t* sweep_launches, double* sweep_bytes,
+                           int32_t reset) {
+    vbd::clear_error();
+    if (!s) VBD_FAIL(VBD_ERR_INVALID_ARG, "null solver handle");
+    DeviceScope scope(s->device);
+    VBD_TRY(s->collect_timing());
+    if (sweep_ms) *sweep_ms = s->timed_ms;
+    if (sweep_launches) *sweep_launches = s->timed_launches;
+    if (sweep_bytes) *sweep_bytes = s->timed_bytes;
+    if (reset) {
+        s->timed_ms = 0.0;
+        s->timed_bytes = 0.0;
+        s->timed_launches = 0;
+    }
+    return VBD_OK;
+}
+
+int vbd_solver_kernel_launches(vbd_solver* s, int64_t* launches) {
+    vbd::clear_error();
+    if (!s || !launches) VBD_FAIL(VBD_ERR_INVALID_ARG, "null argument");
+    *launches = s->launches;
+    return VBD_OK;
+}
+
+}  // extern "C"
