@@ -149,8 +149,14 @@ int vbd_solver_solve_iteration(vbd_solver* s, float dt_sqr_reciprocal);
 int vbd_solver_step(vbd_solver* s, float dt, int32_t substeps, int32_t iterations, const float* gravity,
                     int32_t use_acceleration, float rho);
 
-/* Waits for all work queued on the handle's stream and reports sticky device errors. */
+/* Waits for all work queued on the handle's stream and reports sticky device errors, and
+ * VBD_ERR_TIMEOUT if a grid barrier of the persistent kernel gave up since the last sync. */
 int vbd_solver_sync(vbd_solver* s);
+
+/* Failure-detection self-test: launches the persistent kernel with one barrier arrival missing and
+ * a poll limit of spin_limit, so its first grid barrier can never complete.  Every block gives up
+ * after spin_limit polls and exits; *timed_out receives 1 if the device recorded the timeout. */
+int vbd_solver_barrier_selftest(vbd_solver* s, int64_t spin_limit, int32_t* timed_out);
 
 /* Energies (FP64 accumulation over the FP32 state).  Completes before returning.
  *   VBD_ENERGY_IP:      incremental potential sum_i m_i/(2h^2)|x_i - y_i|^2 + sum_t V_t psi(F_t),
@@ -173,20 +179,38 @@ int vbd_solver_energy(vbd_solver* s, int32_t kind, float h, double* out);
 int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite, int32_t reset);
 
 /* Tuning knobs (all have measured defaults).
- *   VBD_OPT_LANES:       threads cooperating on one vertex: 4, 8, 16 or 32
+ *   VBD_OPT_LANES:       threads cooperating on one vertex: 1, 2, 4, 8, 16 or 32
  *   VBD_OPT_LAYOUT:      0 = tet records gathered through a per-vertex tet list,
  *                        1 = incidence records streamed in colour order
  *   VBD_OPT_GRAPH:       1 = replay a captured CUDA graph per step, 0 = direct launches
  *   VBD_OPT_KERNEL_TIMING: 1 = launch directly and bracket every colour-sweep kernel with a CUDA
- *                        event pair on the handle's stream (read with vbd_solver_kernel_time) */
+ *                        event pair on the handle's stream (read with vbd_solver_kernel_time)
+ *   VBD_OPT_PREFETCH:    1 = load the next element record while evaluating the current one
+ *   VBD_OPT_PDL:         1 = launch colour sweeps with programmatic dependent launch, so a sweep
+ *                        loads its element data while the previous sweep drains
+ *   VBD_OPT_BLOCK:       threads per block of the sweep kernel: 64, 128 or 256
+ *   VBD_OPT_PERSISTENT:  1 = run each step / solve as one cooperative launch that walks the colours
+ *                        with a grid barrier after each one (bounded wait: a barrier that gives up
+ *                        makes the next vbd_solver_sync return VBD_ERR_TIMEOUT) */
 typedef enum vbd_option {
     VBD_OPT_LANES = 0,
     VBD_OPT_LAYOUT = 1,
     VBD_OPT_GRAPH = 2,
-    VBD_OPT_KERNEL_TIMING = 3
+    VBD_OPT_KERNEL_TIMING = 3,
+    VBD_OPT_PREFETCH = 4,
+    VBD_OPT_PDL = 5,
+    VBD_OPT_BLOCK = 6,
+    VBD_OPT_PERSISTENT = 7
 } vbd_option;
 int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value);
 int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value);
+
+/* Autotuner: times `repeats` steps of `iterations` sweeps (dt, no gravity, Chebyshev 0.9) for each
+ * launch shape in a fixed candidate list -- threads per vertex, record layout, prefetch, programmatic
+ * dependent launch, block size -- keeps the fastest, and restores the simulation state (positions,
+ * velocities, inertia, counters) it started from.  chosen (may be null) receives 5 ints:
+ * lanes, layout, prefetch, pdl, block. */
+int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t repeats, int32_t* chosen);
 
 /* Sizes of the uploaded mesh: vertices, tets, colours. */
 int vbd_solver_info(vbd_solver* s, int32_t* num_verts, int32_t* num_tets, int32_t* num_colours);

@@ -10,17 +10,22 @@ def rel_err(a, b, mesh):
 
 
 def gpu_simulate(mesh, steps, dt, iterations, gravity=(0.0, -9.8, 0.0), use_acceleration=True, rho=0.95,
-                 substeps=1, lanes=None, layout=None, graph=None, device=0):
+                 substeps=1, lanes=None, layout=None, graph=None, device=0, options=None):
     s = build_solver(mesh, device=device, lanes=lanes, layout=layout, graph=graph)
+    for k, v in (options or {}).items():
+        s.set_option(k, v)
     try:
+        l0 = s.kernel_launches()
         for _ in range(steps):
             s.step(dt, iterations, gravity, use_acceleration, rho, substeps)
+        s.sync()
+        launches = s.kernel_launches() - l0
         x = s.get_positions()
         v = s.get_velocities()
         h = dt / substeps
         ip = s.energy(0, h)
         sing, nonf = s.status()
-        return dict(x=x, v=v, ip=ip, singular=sing, nonfinite=nonf, launches=s.kernel_launches())
+        return dict(x=x, v=v, ip=ip, singular=sing, nonfinite=nonf, launches=launches)
     finally:
         s.close()
 

@@ -222,3 +222,36 @@ def test_launch_count_reported(gpu_device):
     colour_of, _, _ = color_vertices(m.num_verts, m.tets)
     swept = len(np.unique(colour_of[m.fixed == 0]))
     assert s.kernel_launches() - before == 4 * swept + 2
+
+
+def test_barrier_timeout_is_reported_not_hung(gpu_device):
+    """A grid barrier that can never complete gives up after its poll limit (no hang, no fault)."""
+    m = small_block(seed=42)
+    s = build_solver(m)
+    import ctypes as C
+
+    out = C.c_int32(0)
+    _capi.call("vbd_solver_barrier_selftest", s._h, 2000, C.byref(out))
+    assert out.value == 1
+    # the context stays usable
+    s.set_option(_capi.OPT_PERSISTENT, 1)
+    s.step(1 / 60, 4, (0, -9.8, 0), True, 0.9)
+    s.sync()
+    x = s.get_positions()
+    assert np.all(np.isfinite(x))
+
+
+def test_autotune_restores_state_and_keeps_parity(gpu_device):
+    m = meshgen.cube(12)
+    s = build_solver(m)
+    x0 = s.get_positions()
+    v0 = s.get_velocities()
+    chosen = s.autotune(1 / 120, iterations=5, repeats=1)
+    assert chosen["lanes"] in (2, 4, 8, 16) and chosen["layout"] in (0, 1)
+    np.testing.assert_array_equal(s.get_positions(), x0)
+    np.testing.assert_array_equal(s.get_velocities(), v0)
+    assert s.status() == (0, False)
+    st = meshgen.CUBE_SETTINGS
+    s.step(st["dt"], 10, st["gravity"], True, st["rho"])
+    o = po.simulate(m, 1, st["dt"], 10, st["gravity"], True, st["rho"], precision=32, mode=po.CLOSED)
+    assert rel_err(s.get_positions(), o["x"], m) < 1e-5

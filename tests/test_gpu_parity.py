@@ -10,7 +10,7 @@ import pytest
 
 from helpers import gpu_simulate, rel_err, small_block
 from oracle import pyoracle as po
-from vbd_tetmesh_b200 import meshgen
+from vbd_tetmesh_b200 import _capi, meshgen
 
 pytestmark = pytest.mark.gpu
 
@@ -49,13 +49,47 @@ def test_beam_100_steps_stays_close(gpu_device):
     assert err < 1e-4
 
 
-@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+@pytest.mark.parametrize("lanes", [1, 2, 4, 8, 16, 32])
 @pytest.mark.parametrize("layout", [0, 1])
 def test_launch_shapes_agree(gpu_device, lanes, layout):
     m = small_block(seed=lanes + layout)
     g = gpu_simulate(m, 3, 1 / 60, 15, (0.0, -9.8, 0.0), True, 0.9, lanes=lanes, layout=layout)
     o = po.simulate(m, 3, 1 / 60, 15, (0.0, -9.8, 0.0), True, 0.9, precision=32)
     assert rel_err(g["x"], o["x"], m) < POS_TOL
+
+
+@pytest.mark.parametrize("prefetch,pdl,block", [(0, 0, 256), (1, 0, 128), (0, 1, 64), (1, 1, 128), (1, 1, 256)])
+def test_prefetch_pdl_block_variants(gpu_device, prefetch, pdl, block):
+    m = small_block(seed=prefetch + 2 * pdl + block)
+    opts = {_capi.OPT_PREFETCH: prefetch, _capi.OPT_PDL: pdl, _capi.OPT_BLOCK: block}
+    g = gpu_simulate(m, 3, 1 / 60, 15, (0.0, -9.8, 0.0), True, 0.9, options=opts)
+    o = po.simulate(m, 3, 1 / 60, 15, (0.0, -9.8, 0.0), True, 0.9, precision=32)
+    assert rel_err(g["x"], o["x"], m) < POS_TOL
+    # prefetch, PDL and block size change no arithmetic: bit-identical to the defaults
+    d = gpu_simulate(m, 3, 1 / 60, 15, (0.0, -9.8, 0.0), True, 0.9)
+    np.testing.assert_array_equal(g["x"], d["x"])
+
+
+@pytest.mark.parametrize("lanes,layout", [(4, 0), (8, 1), (16, 1), (32, 0)])
+@pytest.mark.parametrize("accel,substeps", [(True, 1), (False, 2)])
+def test_persistent_kernel_bit_identical(gpu_device, lanes, layout, accel, substeps):
+    m = small_block(seed=lanes + layout, dims=(9, 5, 4), per_tet_sigma=0.2)
+    kw = dict(lanes=lanes, layout=layout, options={_capi.OPT_PREFETCH: 1})
+    a = gpu_simulate(m, 4, 1 / 60, 12, (0.0, -9.8, 0.0), accel, 0.9, substeps=substeps, **kw)
+    kw["options"] = {_capi.OPT_PREFETCH: 1, _capi.OPT_PERSISTENT: 1}
+    b = gpu_simulate(m, 4, 1 / 60, 12, (0.0, -9.8, 0.0), accel, 0.9, substeps=substeps, **kw)
+    np.testing.assert_array_equal(a["x"], b["x"])
+    np.testing.assert_array_equal(a["v"], b["v"])
+    assert b["launches"] == 4 * substeps  # one cooperative launch per sub-step
+
+
+def test_persistent_cube_matches_graph_path(gpu_device):
+    m = meshgen.cube(24)
+    s = meshgen.CUBE_SETTINGS
+    a = gpu_simulate(m, 3, s["dt"], s["iterations"], s["gravity"], True, s["rho"], lanes=8, layout=1)
+    b = gpu_simulate(m, 3, s["dt"], s["iterations"], s["gravity"], True, s["rho"], lanes=8, layout=1,
+                     options={_capi.OPT_PERSISTENT: 1})
+    np.testing.assert_array_equal(a["x"], b["x"])
 
 
 @pytest.mark.parametrize("graph", [0, 1])

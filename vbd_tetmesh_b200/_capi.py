@@ -32,6 +32,10 @@ OPT_LANES = 0
 OPT_LAYOUT = 1
 OPT_GRAPH = 2
 OPT_KERNEL_TIMING = 3
+OPT_PREFETCH = 4
+OPT_PDL = 5
+OPT_BLOCK = 6
+OPT_PERSISTENT = 7
 
 _p = C.c_void_p
 _i32 = C.c_int32
@@ -69,6 +73,8 @@ SIGNATURES = {
     "vbd_solver_info": [_p, _PI32, _PI32, _PI32],
     "vbd_solver_kernel_launches": [_p, _PI64],
     "vbd_solver_kernel_time": [_p, _PF64, _PI64, _PF64, _i32],
+    "vbd_solver_autotune": [_p, _f32, _i32, _i32, _p],
+    "vbd_solver_barrier_selftest": [_p, C.c_int64, _PI32],
 }
 
 _lib = None

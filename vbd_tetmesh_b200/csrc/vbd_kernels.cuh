@@ -29,11 +29,11 @@ struct __align__(16) TetRec {
 };
 static_assert(sizeof(TetRec) == 64, "TetRec must be 64 bytes");
 
-enum StatusSlot { ST_SINGULAR = 0, ST_NONFINITE = 1, ST_SLOTS = 4 };
+enum StatusSlot { ST_SINGULAR = 0, ST_NONFINITE = 1, ST_TIMEOUT = 2, ST_SLOTS = 4 };
 
 struct SweepParams {
     float4* x;                 // positions being swept in place (Gauss-Seidel)
-    float4* xnext;             // receives the Chebyshev-blended position (ACCEL)
+    float4* xnext;             // receives the Chebyshev-blended position (when accel)
     float4* pp;                // position before the previous sweep
     const float4* y;           // inertial target, w = mass
     const int* inc_off;
@@ -44,7 +44,15 @@ struct SweepParams {
     int v_begin, v_end;
     float dtsr;                // 1/h^2
     float omega;
+    int accel;                 // write x^(k) = omega (x~ - pp) + pp to xnext (VBD.cpp:290-300)
+    int keep_pp;               // store the pre-sweep position into pp (VBD.cpp:78,89)
 };
+
+// Programmatic dependent launch: let the next kernel in the stream start its prologue now, and
+// wait until every kernel before this one has finished and its writes are visible.  Both are
+// no-ops for a kernel launched without the programmatic-serialization attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 __device__ __forceinline__ TetRec load_rec(const TetRec* p) {
     TetRec r;
@@ -77,14 +85,22 @@ struct Acc {
 //   Hessian   H_nn = V (mu |q|^2 I + lambda (C q)(C q)^T)   -- the (n,n) block of the literal
 //   12x12 assembly; the cofactor-derivative terms vanish in that block because dC_ij/dF_kl is
 //   antisymmetric in (j,l) and is contracted with the symmetric q q^T.
-template <bool WANT_H>
+// Position loads: the read-only path when positions cannot change while the kernel runs (one
+// colour per launch), plain coherent loads inside the persistent kernel, where other blocks
+// rewrite them between grid barriers.
+template <bool COHERENT> __device__ __forceinline__ float4 load_pos(const float4* X, int i) {
+    if (COHERENT) return X[i];
+    return __ldg(X + i);
+}
+
+template <bool WANT_H, bool COHERENT = false>
 __device__ __forceinline__ void tet_contrib(const TetRec& r, int v, float4 xi, const float4* __restrict__ X,
                                             Acc& acc) {
     const int i0 = r.ids.x, i1 = r.ids.y, i2 = r.ids.z, i3 = r.ids.w;
-    const float4 p0 = (i0 == v) ? xi : __ldg(X + i0);
-    const float4 p1 = (i1 == v) ? xi : __ldg(X + i1);
-    const float4 p2 = (i2 == v) ? xi : __ldg(X + i2);
-    const float4 p3 = (i3 == v) ? xi : __ldg(X + i3);
+    const float4 p0 = (i0 == v) ? xi : load_pos<COHERENT>(X, i0);
+    const float4 p1 = (i1 == v) ? xi : load_pos<COHERENT>(X, i1);
+    const float4 p2 = (i2 == v) ? xi : load_pos<COHERENT>(X, i2);
+    const float4 p3 = (i3 == v) ? xi : load_pos<COHERENT>(X, i3);
     const int n = (i0 == v) ? 0 : (i1 == v) ? 1 : (i2 == v) ? 2 : 3;
 
     const float D00 = r.a.x, D01 = r.a.y, D02 = r.a.z, D10 = r.a.w;
@@ -172,31 +188,36 @@ __device__ __forceinline__ void group_reduce(Acc& a) {
     }
 }
 
-// One colour of one Gauss-Seidel sweep (VBDsolver::solve, VBD.cpp:114-158, and solveVertex
-// :160-203): LANES threads per vertex split its incident tets, reduce with warp shuffles, and
-// the group's first lane solves (m/h^2 I + sum H_nn) dx = m/h^2 (y - x) - sum g_n with the
-// adjugate formula behind the |det| > 1e-8 guard (VBD.cpp:141-152, Types.h:85-112).
-//   STREAM : element records read from the incidence-ordered copy instead of through inc_tet
-//   ACCEL  : also write x^(k) = omega (x~ - pp) + pp to xnext (VBD.cpp:290-300)
-//   KEEP_PP: store the pre-sweep position into pp (VBD.cpp:78,89)
-template <int LANES, bool STREAM, bool ACCEL, bool KEEP_PP>
-__global__ void __launch_bounds__(256) k_sweep(SweepParams p) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & (LANES - 1);
-    const int v = p.v_begin + t / LANES;
-    const bool active = v < p.v_end;
-    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
-    int j0 = 0, j1 = 0;
-    if (active) {
-        xi = p.x[v];
-        j0 = __ldg(p.inc_off + v);
-        j1 = __ldg(p.inc_off + v + 1);
-    }
+template <bool STREAM>
+__device__ __forceinline__ TetRec fetch_rec(const SweepParams& p, int j) {
+    return STREAM ? load_rec(p.irec + j) : load_rec(p.rec + __ldg(p.inc_tet + j));
+}
+
+// The vertex block update of VBDsolver::solveVertex + solve (VBD.cpp:124-203) for vertex v:
+// LANES threads split its incident tets, reduce with warp shuffles, and the group's first lane
+// solves (m/h^2 I + sum H_nn) dx = m/h^2 (y - x) - sum g_n with the adjugate formula behind the
+// |det| > 1e-8 guard (VBD.cpp:141-152, Types.h:85-112), then writes x~, the Chebyshev blend
+// x^(k) = omega (x~ - pp) + pp (VBD.cpp:290-300) and the pre-sweep position into pp.
+// Every lane of the warp must call it (shuffles); `active` marks lanes with a real vertex.
+//   STREAM   : element records read from the incidence-ordered copy instead of through inc_tet
+//   PREFETCH : the next element record is loaded while the current one is evaluated
+//   COHERENT : positions read with coherent loads (persistent kernel)
+// `nxt` holds the lane's first record if PREFETCH (fetched by the caller).
+template <int LANES, bool STREAM, bool PREFETCH, bool COHERENT>
+__device__ __forceinline__ void vertex_update(const SweepParams& p, int v, int lane, bool active, int j, int j1,
+                                              TetRec nxt) {
+    const float4 xi = active ? p.x[v] : make_float4(0.f, 0.f, 0.f, 0.f);
     Acc acc;
     acc.zero();
-    for (int j = j0 + lane; j < j1; j += LANES) {
-        const TetRec r = STREAM ? load_rec(p.irec + j) : load_rec(p.rec + __ldg(p.inc_tet + j));
-        tet_contrib<true>(r, v, xi, p.x, acc);
+    for (; j < j1; j += LANES) {
+        TetRec r;
+        if (PREFETCH) {
+            r = nxt;
+            if (j + LANES < j1) nxt = fetch_rec<STREAM>(p, j + LANES);
+        } else {
+            r = fetch_rec<STREAM>(p, j);
+        }
+        tet_contrib<true, COHERENT>(r, v, xi, p.x, acc);
     }
     group_reduce<LANES>(acc);
     if (!active || lane != 0) return;
@@ -227,7 +248,7 @@ __global__ void __launch_bounds__(256) k_sweep(SweepParams p) {
     }
     if (!(isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z))) p.status[ST_NONFINITE] = 1ull;
     p.x[v] = xn;
-    if (ACCEL) {
+    if (p.accel) {
         const float4 q = p.pp[v];
         float4 xa;
         xa.x = p.omega * (xn.x - q.x) + q.x;
@@ -236,7 +257,187 @@ __global__ void __launch_bounds__(256) k_sweep(SweepParams p) {
         xa.w = xn.w;
         p.xnext[v] = xa;
     }
-    if (KEEP_PP) p.pp[v] = xi;
+    if (p.keep_pp) p.pp[v] = xi;
+}
+
+// One colour of one Gauss-Seidel sweep per launch (VBDsolver::solve, VBD.cpp:114-158).  Element
+// data never changes during a sweep, so the lane's first record is fetched before the dependency
+// wait; positions are read only after it.
+template <int LANES, bool STREAM, bool PREFETCH>
+__global__ void __launch_bounds__(256) k_sweep(SweepParams p) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = LANES == 1 ? 0 : (threadIdx.x & (LANES - 1));
+    const int v = p.v_begin + t / LANES;
+    const bool active = v < p.v_end;
+    int j0 = 0, j1 = 0;
+    if (active) {
+        j0 = __ldg(p.inc_off + v);
+        j1 = __ldg(p.inc_off + v + 1);
+    }
+    const int j = j0 + lane;
+    TetRec nxt;
+    if (PREFETCH && j < j1) nxt = fetch_rec<STREAM>(p, j);
+    pdl_trigger();
+    pdl_wait();
+    vertex_update<LANES, STREAM, PREFETCH, false>(p, v, lane, active, j, j1, nxt);
+}
+
+// ---- persistent colour-walking kernel -------------------------------------------------------
+
+struct GridBarrier {
+    unsigned int count;
+    unsigned int gen;
+};
+
+struct PersistParams {
+    SweepParams sw;           // dtsr, y, element data, status; x / xnext / accel / omega set per sweep
+    float4* xa;               // position buffers (positions start and end in xa)
+    float4* xb;
+    float4* v;
+    float4* xprev;
+    const int* cstart;        // colour c = internal ids [cstart[c], cstart[c+1])
+    const float* omega;       // Chebyshev weight of each iteration (1 = no blend)
+    GridBarrier* bar;
+    long long spin_limit;     // polls of the barrier flag before giving up
+    int ncol, iters, nfree, n;
+    int predict;              // run the inertial predictor first
+    int finish;               // run the velocity update last
+    int init_from_inertia;    // start from x = y
+    int expected_blocks;      // arrivals the barrier waits for (gridDim.x in normal use)
+    float h, hgx, hgy, hgz;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid-wide barrier of a cooperative launch with a bounded wait: after spin_limit polls the
+// waiting block records ST_TIMEOUT and the call returns false (the caller then exits), so a
+// barrier that can never complete ends the kernel instead of hanging it.
+__device__ __forceinline__ bool grid_barrier(GridBarrier* bar, int expected, long long spin_limit,
+                                             unsigned long long* status) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned gen = ld_acquire_gpu(&bar->gen);
+        __threadfence();
+        const unsigned arrived = atomicAdd(&bar->count, 1u);
+        if (arrived == (unsigned)expected - 1u) {
+            bar->count = 0u;
+            __threadfence();
+            st_release_gpu(&bar->gen, gen + 1u);
+        } else {
+            long long polls = 0;
+            while (ld_acquire_gpu(&bar->gen) == gen) {
+                if (++polls > spin_limit) {
+                    ok = 0;
+                    atomicOr(reinterpret_cast<unsigned int*>(status + ST_TIMEOUT), 1u);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Whole step (or solve) in one cooperative launch: predictor, `iters` sweeps over the colours
+// with a grid barrier after each colour, velocity update.  Same arithmetic as k_predict /
+// k_sweep / k_finish, so results are bit-identical to the multi-launch path.
+template <int LANES, bool STREAM>
+__global__ void __launch_bounds__(256, 4) k_persistent(PersistParams p) {
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nthreads = gridDim.x * blockDim.x;
+    if (p.predict) {
+        for (int i = gtid; i < p.n; i += nthreads) {
+            const float4 xi = p.xa[i];
+            p.xprev[i] = xi;
+            float4 yi = p.sw.y[i];
+            if (i < p.nfree) {
+                float4 vi = p.v[i];
+                vi.x += p.hgx;
+                vi.y += p.hgy;
+                vi.z += p.hgz;
+                p.v[i] = vi;
+                yi.x = xi.x + p.h * vi.x;
+                yi.y = xi.y + p.h * vi.y;
+                yi.z = xi.z + p.h * vi.z;
+            } else {
+                yi.x = xi.x;
+                yi.y = xi.y;
+                yi.z = xi.z;
+            }
+            const_cast<float4*>(p.sw.y)[i] = yi;
+        }
+    }
+    if (p.init_from_inertia) {
+        for (int i = gtid; i < p.n; i += nthreads) {
+            const float4 yi = p.sw.y[i];
+            float4 a = p.xa[i], b = p.xb[i];
+            a.x = b.x = yi.x;
+            a.y = b.y = yi.y;
+            a.z = b.z = yi.z;
+            p.xa[i] = a;
+            p.xb[i] = b;
+        }
+    }
+    if (!grid_barrier(p.bar, p.expected_blocks, p.spin_limit, p.sw.status)) return;
+
+    const int lane_w = threadIdx.x & 31;
+    const int lane = LANES == 1 ? 0 : (lane_w & (LANES - 1));
+    const int groups_per_warp = 32 / LANES;
+    const int warp = gtid >> 5;
+    const int nwarps = nthreads >> 5;
+    int cur = 0;
+    SweepParams sp = p.sw;
+    for (int k = 0; k < p.iters; ++k) {
+        const float om = p.omega[k];
+        const bool blend = om > 1.0f;
+        sp.x = cur ? p.xb : p.xa;
+        sp.xnext = cur ? p.xa : p.xb;
+        sp.omega = om;
+        sp.accel = blend ? 1 : 0;
+        for (int c = 0; c < p.ncol; ++c) {
+            const int vb = p.cstart[c], ve = p.cstart[c + 1];
+            for (int base = vb + warp * groups_per_warp; base < ve; base += nwarps * groups_per_warp) {
+                const int v = base + lane_w / LANES;
+                const bool active = v < ve;
+                int j0 = 0, j1 = 0;
+                if (active) {
+                    j0 = __ldg(sp.inc_off + v);
+                    j1 = __ldg(sp.inc_off + v + 1);
+                }
+                const int j = j0 + lane;
+                TetRec nxt;
+                if (j < j1) nxt = fetch_rec<STREAM>(sp, j);
+                vertex_update<LANES, STREAM, true, true>(sp, v, lane, active, j, j1, nxt);
+            }
+            if (!grid_barrier(p.bar, p.expected_blocks, p.spin_limit, p.sw.status)) return;
+        }
+        if (blend) cur ^= 1;
+    }
+    for (int i = gtid; i < p.nfree; i += nthreads) {
+        const float4 xf = cur ? p.xb[i] : p.xa[i];
+        if (cur) p.xa[i] = xf;
+        if (p.finish) {
+            const float4 xp = p.xprev[i];
+            float4 vi = p.v[i];
+            vi.x = ((xf.x - xp.x) / p.h) * 0.999f;
+            vi.y = ((xf.y - xp.y) / p.h) * 0.999f;
+            vi.z = ((xf.z - xp.z) / p.h) * 0.999f;
+            p.v[i] = vi;
+        }
+    }
 }
 
 // Inertial predictor (VBDsolver::forwardStep, VBD.cpp:103-112; TetMesh::applyGravity /

@@ -60,30 +60,26 @@ static float omega_of(int order, float rho, float prev) {
 
 using SweepFn = void (*)(SweepParams);
 
-template <int L, bool S, bool A, bool K> static SweepFn sweep_fn() { return &k_sweep<L, S, A, K>; }
-
-template <int L> static SweepFn pick_sweep(bool stream, bool accel, bool keep) {
-    if (stream) {
-        if (accel) return keep ? sweep_fn<L, true, true, true>() : sweep_fn<L, true, true, false>();
-        return keep ? sweep_fn<L, true, false, true>() : sweep_fn<L, true, false, false>();
-    }
-    if (accel) return keep ? sweep_fn<L, false, true, true>() : sweep_fn<L, false, true, false>();
-    return keep ? sweep_fn<L, false, false, true>() : sweep_fn<L, false, false, false>();
+template <int L> static SweepFn pick_sweep(bool stream, bool prefetch) {
+    if (stream) return prefetch ? &k_sweep<L, true, true> : &k_sweep<L, true, false>;
+    return prefetch ? &k_sweep<L, false, true> : &k_sweep<L, false, false>;
 }
 
-static SweepFn pick_sweep(int lanes, bool stream, bool accel, bool keep) {
+static SweepFn pick_sweep(int lanes, bool stream, bool prefetch) {
     switch (lanes) {
-        case 4: return pick_sweep<4>(stream, accel, keep);
-        case 8: return pick_sweep<8>(stream, accel, keep);
-        case 16: return pick_sweep<16>(stream, accel, keep);
-        default: return pick_sweep<32>(stream, accel, keep);
+        case 1: return pick_sweep<1>(stream, prefetch);
+        case 2: return pick_sweep<2>(stream, prefetch);
+        case 4: return pick_sweep<4>(stream, prefetch);
+        case 8: return pick_sweep<8>(stream, prefetch);
+        case 16: return pick_sweep<16>(stream, prefetch);
+        default: return pick_sweep<32>(stream, prefetch);
     }
 }
 
 // Key of a captured step / solve graph: everything baked into its kernel parameters.
 struct GraphKey {
     int kind;  // 0 = step, 1 = solve, 2 = single sweep
-    int iters, accel, init, lanes, layout;
+    int iters, accel, init, lanes, layout, prefetch, pdl, block;
     float h, dtsr, hg[3], rho;
     bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
 };
@@ -111,7 +107,15 @@ struct vbd_solver {
     vbd::DBuf<float> stage, mat_stage;
     vbd::DBuf<unsigned long long> status;
     vbd::DBuf<double> partials, scalar;
-    int lanes = 8, layout = 0, use_graph = 1, timing = 0;
+    // defaults: the fastest shape measured on the 64^3 cube (streamed records, 8 lanes per vertex,
+    // record prefetch, programmatic dependent launch, 128-thread blocks)
+    int lanes = 8, layout = 1, use_graph = 1, timing = 0, prefetch = 1, pdl = 1, block = 128;
+    int persistent = 0;                             // whole step in one cooperative launch
+    long long spin_limit = 1LL << 22;               // barrier polls before a persistent launch gives up
+    vbd::DBuf<int> d_cstart;
+    vbd::DBuf<float> d_omega;
+    vbd::DBuf<vbd::GridBarrier> barrier;
+    std::vector<float> omega_cache;
     long long launches = 0;
     std::vector<vbd::GraphEntry> graphs;
     std::vector<double> colour_bytes;               // algorithmic bytes of one sweep of colour c
@@ -175,16 +179,26 @@ struct vbd_solver {
     int launch_sweep(int c, float4* xr, float4* xn, bool accel, bool keep_pp, float dtsr, float omega) {
         const int vb = cstart[c], ve = cstart[c + 1];
         if (ve <= vb) return VBD_OK;
-        vbd::SweepParams p{xr,        xn,    pp.p,        y.p,  inc_off.p, inc_tet.p, rec.p,
-                           irec.p,    status.p, vb,       ve,   dtsr,      omega};
+        vbd::SweepParams p{xr,   xn, pp.p, y.p,   inc_off.p,     inc_tet.p,         rec.p,
+                           irec.p, status.p, vb, ve, dtsr, omega, accel ? 1 : 0, keep_pp ? 1 : 0};
         const long long threads = (long long)(ve - vb) * lanes;
-        vbd::SweepFn fn = vbd::pick_sweep(lanes, layout == 1, accel, keep_pp);
+        vbd::SweepFn fn = vbd::pick_sweep(lanes, layout == 1, prefetch != 0);
         cudaEvent_t ev[2] = {nullptr, nullptr};
         if (timing) {
             VBD_TRY(timing_event(ev));
             CUDA_TRY(cudaEventRecord(ev[0], stream));
         }
-        fn<<<vbd::nblk(threads, 256), 256, 0, stream>>>(p);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(vbd::nblk(threads, block));
+        cfg.blockDim = dim3(block);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = (pdl && !timing) ? 1 : 0;
+        CUDA_TRY(cudaLaunchKernelEx(&cfg, fn, p));
         VBD_TRY(check_launch());
         if (timing) {
             CUDA_TRY(cudaEventRecord(ev[1], stream));
@@ -237,6 +251,74 @@ struct vbd_solver {
             VBD_TRY(check_launch());
         }
         return VBD_OK;
+    }
+
+    // Chebyshev weights of `iters` iterations (1 where no blend happens).
+    std::vector<float> omega_schedule(int iters, bool accel, float rho) const {
+        std::vector<float> w(std::max(iters, 1), 1.0f);
+        float omega = 1.0f;
+        for (int k = 1; k <= iters; ++k) {
+            if (accel) omega = vbd::omega_of(k, rho, omega);
+            w[k - 1] = accel ? omega : 1.0f;
+        }
+        return w;
+    }
+
+    int launch_persistent(int iters, float dtsr, bool accel, float rho, bool predict, bool finish, bool from_inertia,
+                          float h, const float* hg, int expected_extra = 0) {
+        if (!barrier.p) VBD_TRY(barrier.alloc(1));
+        if (d_cstart.n != cstart.size()) {
+            VBD_TRY(d_cstart.alloc(cstart.size()));
+            CUDA_TRY(cudaMemcpy(d_cstart.p, cstart.data(), sizeof(int) * cstart.size(), cudaMemcpyHostToDevice));
+        }
+        std::vector<float> w = omega_schedule(iters, accel, rho);
+        if (w != omega_cache) {
+            if (d_omega.n < w.size()) VBD_TRY(d_omega.alloc(w.size()));
+            CUDA_TRY(cudaMemcpyAsync(d_omega.p, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice, stream));
+            CUDA_TRY(cudaStreamSynchronize(stream));
+            omega_cache = w;
+        }
+        const int L = lanes < 4 ? 4 : lanes;
+        void (*fn)(vbd::PersistParams) = nullptr;
+        const bool st = layout == 1;
+        switch (L) {
+            case 4: fn = st ? &vbd::k_persistent<4, true> : &vbd::k_persistent<4, false>; break;
+            case 8: fn = st ? &vbd::k_persistent<8, true> : &vbd::k_persistent<8, false>; break;
+            case 16: fn = st ? &vbd::k_persistent<16, true> : &vbd::k_persistent<16, false>; break;
+            default: fn = st ? &vbd::k_persistent<32, true> : &vbd::k_persistent<32, false>; break;
+        }
+        int per_sm = 0, sms = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0));
+        CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        if (per_sm < 1) VBD_FAIL(VBD_ERR_CUDA, "persistent kernel cannot be resident");
+        const int grid = per_sm * sms;
+        vbd::PersistParams pp_{};
+        pp_.sw = vbd::SweepParams{x0.p, x1.p, pp.p,   y.p,  inc_off.p, inc_tet.p, rec.p, irec.p,
+                                  status.p, 0, 0,     dtsr, 1.0f, 0, accel ? 1 : 0};
+        pp_.xa = x0.p;
+        pp_.xb = x1.p;
+        pp_.v = v.p;
+        pp_.xprev = xprev.p;
+        pp_.cstart = d_cstart.p;
+        pp_.omega = d_omega.p;
+        pp_.bar = barrier.p;
+        pp_.spin_limit = spin_limit;
+        pp_.ncol = C;
+        pp_.iters = iters;
+        pp_.nfree = nfree;
+        pp_.n = N;
+        pp_.predict = predict ? 1 : 0;
+        pp_.finish = finish ? 1 : 0;
+        pp_.init_from_inertia = from_inertia ? 1 : 0;
+        pp_.expected_blocks = grid + expected_extra;
+        pp_.h = h;
+        pp_.hgx = hg ? hg[0] : 0.f;
+        pp_.hgy = hg ? hg[1] : 0.f;
+        pp_.hgz = hg ? hg[2] : 0.f;
+        CUDA_TRY(cudaMemsetAsync(barrier.p, 0, sizeof(vbd::GridBarrier), stream));
+        void* args[] = {&pp_};
+        CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(fn), dim3(grid), dim3(256), args, 0, stream));
+        return check_launch();
     }
 
     template <class Emit> int run(const vbd::GraphKey& key, Emit emit) {
@@ -511,6 +593,7 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     s->nfree = nfree;
     s->ninc = ninc;
     s->cstart = cstart;
+    s->d_cstart.release();
     s->have_materials = tet_mu != nullptr;
     VBD_TRY(s->repack_stream());
     CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -630,8 +713,14 @@ int vbd_solver_solve(vbd_solver* s, int32_t iterations, float dt_sqr_reciprocal,
     key.init = init_mode;
     key.lanes = s->lanes;
     key.layout = s->layout;
+    key.prefetch = s->prefetch;
+    key.pdl = s->pdl;
+    key.block = s->block;
     key.dtsr = dt_sqr_reciprocal;
     key.rho = rho;
+    if (s->persistent && !s->timing)
+        return s->launch_persistent(iterations, dt_sqr_reciprocal, use_acceleration != 0, rho, false, false,
+                                    init_mode == VBD_INIT_FROM_INERTIA, 1.0f, nullptr);
     return s->run(key, [&] { return s->emit_solve(iterations, dt_sqr_reciprocal, use_acceleration != 0, rho, init_mode); });
 }
 
@@ -665,14 +754,21 @@ int vbd_solver_step(vbd_solver* s, float dt, int32_t substeps, int32_t iteration
     key.accel = use_acceleration ? 1 : 0;
     key.lanes = s->lanes;
     key.layout = s->layout;
+    key.prefetch = s->prefetch;
+    key.pdl = s->pdl;
+    key.block = s->block;
     key.h = h;
     key.dtsr = dtsr;
     key.hg[0] = hg[0];
     key.hg[1] = hg[1];
     key.hg[2] = hg[2];
     key.rho = rho;
-    for (int k = 0; k < substeps; ++k)
-        VBD_TRY(s->run(key, [&] { return s->emit_substep(h, dtsr, hg, iterations, use_acceleration != 0, rho); }));
+    for (int k = 0; k < substeps; ++k) {
+        if (s->persistent && !s->timing)
+            VBD_TRY(s->launch_persistent(iterations, dtsr, use_acceleration != 0, rho, true, true, false, h, hg));
+        else
+            VBD_TRY(s->run(key, [&] { return s->emit_substep(h, dtsr, hg, iterations, use_acceleration != 0, rho); }));
+    }
     return VBD_OK;
 }
 
@@ -681,6 +777,33 @@ int vbd_solver_sync(vbd_solver* s) {
     if (!s) VBD_FAIL(VBD_ERR_INVALID_ARG, "null solver handle");
     DeviceScope scope(s->device);
     CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (s->status.p) {
+        unsigned long long t = 0;
+        CUDA_TRY(cudaMemcpy(&t, s->status.p + vbd::ST_TIMEOUT, sizeof(t), cudaMemcpyDeviceToHost));
+        if (t) {
+            CUDA_TRY(cudaMemset(s->status.p + vbd::ST_TIMEOUT, 0, sizeof(t)));
+            VBD_FAIL(VBD_ERR_TIMEOUT, "a grid barrier of the persistent kernel gave up waiting");
+        }
+    }
+    return VBD_OK;
+}
+
+int vbd_solver_barrier_selftest(vbd_solver* s, int64_t spin_limit, int32_t* timed_out) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!timed_out || spin_limit < 1) VBD_FAIL(VBD_ERR_INVALID_ARG, "need timed_out and spin_limit >= 1");
+    DeviceScope scope(s->device);
+    const long long saved = s->spin_limit;
+    s->spin_limit = spin_limit;
+    // one arrival more than the grid has: the first barrier can never complete
+    int rc = s->launch_persistent(0, 1.0f, false, 0.0f, false, false, false, 1.0f, nullptr, 1);
+    s->spin_limit = saved;
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    unsigned long long t = 0;
+    CUDA_TRY(cudaMemcpy(&t, s->status.p + vbd::ST_TIMEOUT, sizeof(t), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemset(s->status.p + vbd::ST_TIMEOUT, 0, sizeof(t)));
+    *timed_out = t ? 1 : 0;
     return VBD_OK;
 }
 
@@ -699,7 +822,7 @@ int vbd_solver_energy(vbd_solver* s, int32_t kind, float h, double* out) {
         }
         vbd::SweepParams p{s->x0.p, nullptr, s->pp.p, s->y.p, s->inc_off.p, s->inc_tet.p, s->rec.p, s->irec.p,
                            s->status.p, 0, s->nfree, (float)(1.0 / ((double)h * h)), 1.0f};
-        const int L = s->lanes;
+        const int L = std::max(4, s->lanes);
         const unsigned blocks = vbd::nblk((long long)s->nfree * L, 256);
         switch (L) {
             case 4: vbd::k_residual<4><<<blocks, 256, 0, s->stream>>>(p, s->partials.p); break;
@@ -744,9 +867,23 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
     DeviceScope scope(s->device);
     switch (option) {
         case VBD_OPT_LANES:
-            if (value != 4 && value != 8 && value != 16 && value != 32)
-                VBD_FAIL(VBD_ERR_INVALID_ARG, "lanes must be 4, 8, 16 or 32");
+            if (value != 1 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)
+                VBD_FAIL(VBD_ERR_INVALID_ARG, "lanes must be 1, 2, 4, 8, 16 or 32");
             s->lanes = value;
+            return VBD_OK;
+        case VBD_OPT_PREFETCH:
+            s->prefetch = value ? 1 : 0;
+            return VBD_OK;
+        case VBD_OPT_PDL:
+            s->pdl = value ? 1 : 0;
+            return VBD_OK;
+        case VBD_OPT_PERSISTENT:
+            s->persistent = value ? 1 : 0;
+            return VBD_OK;
+        case VBD_OPT_BLOCK:
+            if (value != 64 && value != 128 && value != 256)
+                VBD_FAIL(VBD_ERR_INVALID_ARG, "block must be 64, 128 or 256");
+            s->block = value;
             return VBD_OK;
         case VBD_OPT_LAYOUT:
             if (value != 0 && value != 1) VBD_FAIL(VBD_ERR_INVALID_ARG, "layout must be 0 or 1");
@@ -775,6 +912,10 @@ int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value) {
         case VBD_OPT_LAYOUT: *value = s->layout; return VBD_OK;
         case VBD_OPT_GRAPH: *value = s->use_graph; return VBD_OK;
         case VBD_OPT_KERNEL_TIMING: *value = s->timing; return VBD_OK;
+        case VBD_OPT_PREFETCH: *value = s->prefetch; return VBD_OK;
+        case VBD_OPT_PDL: *value = s->pdl; return VBD_OK;
+        case VBD_OPT_BLOCK: *value = s->block; return VBD_OK;
+        case VBD_OPT_PERSISTENT: *value = s->persistent; return VBD_OK;
         default: VBD_FAIL(VBD_ERR_INVALID_ARG, "unknown option %d", option);
     }
 }
@@ -801,6 +942,93 @@ int vbd_solver_kernel_time(vbd_solver* s, double* sweep_ms, int64_t* sweep_launc
         s->timed_ms = 0.0;
         s->timed_bytes = 0.0;
         s->timed_launches = 0;
+    }
+    return VBD_OK;
+}
+
+int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t repeats, int32_t* chosen) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!s->have_materials) VBD_FAIL(VBD_ERR_STATE, "materials not set");
+    if (!(dt > 0.f) || iterations < 1 || repeats < 1) VBD_FAIL(VBD_ERR_INVALID_ARG, "need dt > 0, iterations >= 1, repeats >= 1");
+    DeviceScope scope(s->device);
+    // Save the state the candidate steps overwrite.
+    const size_t b4 = sizeof(float4) * (size_t)s->N;
+    vbd::DBuf<float4> save;
+    VBD_TRY(save.alloc(6 * (size_t)s->N));
+    float4* bufs[6] = {s->x0.p, s->x1.p, s->pp.p, s->y.p, s->v.p, s->xprev.p};
+    for (int k = 0; k < 6; ++k)
+        CUDA_TRY(cudaMemcpyAsync(save.p + (size_t)k * s->N, bufs[k], b4, cudaMemcpyDeviceToDevice, s->stream));
+    unsigned long long st[vbd::ST_SLOTS];
+    CUDA_TRY(cudaMemcpyAsync(st, s->status.p, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    const int saved_timing = s->timing;
+    s->timing = 0;
+    struct Cand {
+        int lanes, layout, prefetch, pdl, block;
+    };
+    static const Cand cands[] = {
+        {8, 1, 1, 1, 128}, {4, 1, 1, 1, 128}, {8, 1, 1, 0, 128}, {4, 1, 1, 0, 128}, {16, 1, 1, 1, 128},
+        {2, 1, 1, 0, 128}, {8, 0, 1, 1, 128}, {4, 0, 1, 1, 128}, {8, 0, 1, 0, 128}, {4, 0, 1, 0, 128},
+        {8, 1, 1, 1, 256}, {4, 1, 1, 1, 256},
+    };
+    const float g[3] = {0.f, 0.f, 0.f};
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    float best_ms = 1e30f;
+    Cand best = cands[0];
+    int rc = VBD_OK;
+    for (const Cand& c : cands) {
+        s->lanes = c.lanes;
+        s->prefetch = c.prefetch;
+        s->pdl = c.pdl;
+        s->block = c.block;
+        if (s->layout != c.layout) {
+            s->layout = c.layout;
+            if ((rc = s->repack_stream())) break;
+        }
+        // one warm-up step (captures the graph), then the timed ones
+        if ((rc = vbd_solver_step(s, dt, 1, iterations, g, 1, 0.9f))) break;
+        cudaEventRecord(e0, s->stream);
+        for (int r = 0; r < repeats && !rc; ++r) rc = vbd_solver_step(s, dt, 1, iterations, g, 1, 0.9f);
+        cudaEventRecord(e1, s->stream);
+        if (rc) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = VBD_ERR_CUDA;
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+        for (int k = 0; k < 6; ++k)
+            cudaMemcpyAsync(bufs[k], save.p + (size_t)k * s->N, b4, cudaMemcpyDeviceToDevice, s->stream);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    for (int k = 0; k < 6; ++k)
+        CUDA_TRY(cudaMemcpyAsync(bufs[k], save.p + (size_t)k * s->N, b4, cudaMemcpyDeviceToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->status.p, st, sizeof(st), cudaMemcpyHostToDevice, s->stream));
+    s->timing = saved_timing;
+    s->lanes = best.lanes;
+    s->prefetch = best.prefetch;
+    s->pdl = best.pdl;
+    s->block = best.block;
+    if (s->layout != best.layout) {
+        s->layout = best.layout;
+        VBD_TRY(s->repack_stream());
+    }
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (rc) return rc;
+    if (chosen) {
+        chosen[0] = best.lanes;
+        chosen[1] = best.layout;
+        chosen[2] = best.prefetch;
+        chosen[3] = best.pdl;
+        chosen[4] = best.block;
     }
     return VBD_OK;
 }

@@ -212,6 +212,12 @@ class GPUSolver:
         call("vbd_solver_kernel_time", self._h, C.byref(ms), C.byref(n), C.byref(b), int(bool(reset)))
         return ms.value, n.value, b.value
 
+    def autotune(self, dt: float, iterations: int = 10, repeats: int = 2) -> dict:
+        """Times the candidate launch shapes, keeps the fastest and restores the state."""
+        out = (C.c_int32 * 5)()
+        call("vbd_solver_autotune", self._h, float(dt), int(iterations), int(repeats), C.cast(out, C.c_void_p))
+        return dict(zip(("lanes", "layout", "prefetch", "pdl", "block"), list(out)))
+
     def kernel_launches(self) -> int:
         v = C.c_int64(0)
         call("vbd_solver_kernel_launches", self._h, C.byref(v))
