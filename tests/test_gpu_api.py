@@ -255,3 +255,15 @@ def test_autotune_restores_state_and_keeps_parity(gpu_device):
     s.step(st["dt"], 10, st["gravity"], True, st["rho"])
     o = po.simulate(m, 1, st["dt"], 10, st["gravity"], True, st["rho"], precision=32, mode=po.CLOSED)
     assert rel_err(s.get_positions(), o["x"], m) < 1e-5
+
+
+def test_layout_switches_rebuild_captured_graphs(gpu_device):
+    """Switching the record layout frees / reallocates the streamed copy; steps replayed afterwards
+    (same step parameters, so the same graph key) must use the new buffers."""
+    m = small_block(seed=43)
+    s = build_solver(m, layout=1)
+    for layout in (1, 0, 1, 0, 1):
+        s.set_option(_capi.OPT_LAYOUT, layout)
+        s.step(1 / 60, 6, (0, -9.8, 0), True, 0.9)
+    o = po.simulate(m, 5, 1 / 60, 6, (0, -9.8, 0), True, 0.9)
+    assert rel_err(s.get_positions(), o["x"], m) < 1e-5

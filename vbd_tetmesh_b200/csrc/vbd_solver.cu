@@ -376,12 +376,20 @@ struct vbd_solver {
         return VBD_OK;
     }
 
+    // Captured graphs bake in buffer addresses: every (re)allocation or release of the streamed
+    // record copy invalidates them.
     int repack_stream() {
         if (layout != 1) {
-            irec.release();
+            if (irec.p) {
+                drop_graphs();
+                irec.release();
+            }
             return VBD_OK;
         }
-        if (irec.n != (size_t)ninc) VBD_TRY(irec.alloc(ninc));
+        if (irec.n != (size_t)ninc) {
+            drop_graphs();
+            VBD_TRY(irec.alloc(ninc));
+        }
         if (ninc > 0) {
             vbd::k_pack_stream<<<vbd::nblk(ninc, 256), 256, 0, stream>>>(rec.p, inc_tet.p, irec.p, (int)ninc);
             VBD_TRY(check_launch());
