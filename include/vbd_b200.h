@@ -212,6 +212,24 @@ int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value);
  * lanes, layout, prefetch, pdl, block. */
 int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t repeats, int32_t* chosen);
 
+/* Allocation-free incremental potential.  No counterpart in the reference: it exists for callers
+ * that cannot let a library allocate device memory -- code embedded in a framework that owns the
+ * device memory (a PyTorch caching-allocator pool, an engine's fixed arena) or in a fixed-latency
+ * loop, where cudaMalloc / cudaFree would synchronise the device or fail once the pool holds the
+ * free memory.  It computes the same quantity as vbd_solver_energy(VBD_ENERGY_IP) from caller-owned
+ * DEVICE arrays in the reference layouts (positions / inertia float[3N], vertex_mass[N], tets
+ * int32[4T], dm_inv float[9T] row-major, rest_vol / tet_mu / tet_lambda float[T]) and writes the
+ * FP64 sum to the device pointer `out`.  It allocates nothing: its scratch (block partials and an
+ * error flag) is a fixed 32 KiB __device__ array that every GPU loading the library holds until
+ * exit, so num_verts + num_tets is limited to 16,777,216 (larger sizes return
+ * VBD_ERR_INVALID_ARG).  The first call on each device looks up the scratch address and must come
+ * before any stream capture on that device.  Calls share the scratch: calls that overlap on the
+ * GPU race.  Runs on `cuda_stream` (null = default stream) and completes before returning; tets
+ * with ids outside [0, N) are skipped and reported as VBD_ERR_INVALID_ARG. */
+int vbd_ip_energy_noalloc(int32_t num_verts, int32_t num_tets, const float* positions, const float* inertia,
+                          const float* vertex_mass, const int32_t* tets, const float* dm_inv, const float* rest_vol,
+                          const float* tet_mu, const float* tet_lambda, float h, double* out, void* cuda_stream);
+
 /* Sizes of the uploaded mesh: vertices, tets, colours. */
 int vbd_solver_info(vbd_solver* s, int32_t* num_verts, int32_t* num_tets, int32_t* num_colours);
 

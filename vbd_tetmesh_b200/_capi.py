@@ -75,6 +75,7 @@ SIGNATURES = {
     "vbd_solver_kernel_time": [_p, _PF64, _PI64, _PF64, _i32],
     "vbd_solver_autotune": [_p, _f32, _i32, _i32, _p],
     "vbd_solver_barrier_selftest": [_p, C.c_int64, _PI32],
+    "vbd_ip_energy_noalloc": [_i32, _i32, _p, _p, _p, _p, _p, _p, _p, _p, _f32, _p, _p],
 }
 
 _lib = None
