@@ -126,7 +126,7 @@ class ClockSampler:
             self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{self.device_index}.csv")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "20"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
@@ -257,7 +257,6 @@ def main():
             e1.synchronize()
             ms_total += e0.elapsed_time(e1)
         barrier()
-        clock_info = clocks.stop()
         launches = solver.kernel_launches() - launches0
 
         # ---- kernel timing pass: event pair around every colour-sweep launch ----
@@ -287,6 +286,8 @@ def main():
                 solver.get_velocities(vh)
             e2e_s = time.perf_counter() - t0
             barrier()
+        # clocks sampled over the three timed passes (device-resident, kernel-timed, e2e)
+        clock_info = clocks.stop()
 
     sing, nonf = solver.status()
     t_max = torch.tensor([ms_total, e2e_s if not args.no_e2e else 0.0], dtype=torch.float64, device=f"cuda:{local}")
