@@ -192,3 +192,88 @@ class Handle:
 
     def __del__(self):
         self.close()
+
+
+# ---- the reference's own sources, compiled against the Eigen-API subset (oracle/_ref) -------------
+
+REF_LIB_PATH = os.path.join(_HERE, "_ref", "libvbdref.so")
+_ref_lib = None
+
+
+def ref_available():
+    return os.path.exists(REF_LIB_PATH)
+
+
+def ref_lib():
+    global _ref_lib
+    if _ref_lib is None:
+        L = C.CDLL(REF_LIB_PATH)
+        f = C.c_float
+        L.ref_create.argtypes = [_i, _i, _p, _p, _p, _p, _p, f, f, f, f, _i, _i, _p, _i, f, _i]
+        L.ref_create.restype = _p
+        L.ref_step.argtypes = [_p, _i]
+        L.ref_step.restype = None
+        L.ref_iterations.argtypes = [_p, _i]
+        L.ref_iterations.restype = None
+        L.ref_state.argtypes = [_p, _p, _p]
+        L.ref_state.restype = None
+        L.ref_setup.argtypes = [_p, _p, _p, _p, _p, _p]
+        L.ref_setup.restype = _i
+        L.ref_energy_history.argtypes = [_p, _p, _i]
+        L.ref_energy_history.restype = _i
+        L.ref_destroy.argtypes = [_p]
+        L.ref_destroy.restype = None
+        _ref_lib = L
+    return _ref_lib
+
+
+class RefHandle:
+    """The reference's TetMesh + VBDsolver (scalar mu / lambda, as VBD.cpp:214-215 uses)."""
+
+    def __init__(self, mesh, dt, iterations, gravity=(0.0, -9.8, 0.0), use_acceleration=True, rho=0.95,
+                 substeps=1, threads=1):
+        f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+        self._keep = [f32(mesh.rest).reshape(-1, 3), f32(mesh.x).reshape(-1, 3), f32(mesh.v).reshape(-1, 3),
+                      np.ascontiguousarray(mesh.tets, dtype=np.int32), np.ascontiguousarray(mesh.fixed, np.uint8),
+                      f32(gravity)]
+        r, x, v, t, fx, g = self._keep
+        self.n, self.t = r.shape[0], t.shape[0]
+        self._h = ref_lib().ref_create(self.n, self.t, _ptr(r), _ptr(x), _ptr(v), _ptr(t), _ptr(fx),
+                                       float(mesh.density), float(mesh.mu[0]), float(mesh.lam[0]), float(dt),
+                                       int(substeps), int(iterations), _ptr(g), int(bool(use_acceleration)),
+                                       float(rho), int(threads))
+
+    def step(self, n=1):
+        ref_lib().ref_step(self._h, int(n))
+
+    def iterations(self, n):
+        ref_lib().ref_iterations(self._h, int(n))
+
+    def state(self):
+        x = np.empty((self.n, 3), np.float32)
+        v = np.empty((self.n, 3), np.float32)
+        ref_lib().ref_state(self._h, _ptr(x), _ptr(v))
+        return x, v
+
+    def setup(self):
+        col = np.empty(self.n, np.int32)
+        mass = np.empty(self.n, np.float32)
+        trv = np.empty(self.t, np.float32)
+        dm = np.empty((self.t, 3, 3), np.float32)
+        v0 = np.empty(self.t, np.float32)
+        nc = ref_lib().ref_setup(self._h, _ptr(col), _ptr(mass), _ptr(trv), _ptr(dm), _ptr(v0))
+        return dict(colour_of=col, ncolours=nc, mass=mass, tet_rest_vol=trv, dminv=dm, v0=v0)
+
+    def energy_history(self):
+        n = ref_lib().ref_energy_history(self._h, None, 0)
+        out = np.empty(max(n, 1))
+        ref_lib().ref_energy_history(self._h, _ptr(out), n)
+        return out[:n]
+
+    def close(self):
+        if self._h:
+            ref_lib().ref_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
