@@ -181,7 +181,9 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
 /* Tuning knobs (all have measured defaults).
  *   VBD_OPT_LANES:       threads cooperating on one vertex: 1, 2, 4, 8, 16 or 32
  *   VBD_OPT_LAYOUT:      0 = tet records gathered through a per-vertex tet list,
- *                        1 = incidence records streamed in colour order
+ *                        1 = 64 B tet records copied into incidence order and streamed,
+ *                        2 = compact 56 B incidence records streamed (other three vertex ids, their
+ *                            rows of Ps Dm^-1, V0 mu, V0 lambda)
  *   VBD_OPT_GRAPH:       1 = replay a captured CUDA graph per step, 0 = direct launches
  *   VBD_OPT_KERNEL_TIMING: 1 = launch directly and bracket every colour-sweep kernel with a CUDA
  *                        event pair on the handle's stream (read with vbd_solver_kernel_time)

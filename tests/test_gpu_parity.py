@@ -50,7 +50,7 @@ def test_beam_100_steps_stays_close(gpu_device):
 
 
 @pytest.mark.parametrize("lanes", [1, 2, 4, 8, 16, 32])
-@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("layout", [0, 1, 2])
 def test_launch_shapes_agree(gpu_device, lanes, layout):
     m = small_block(seed=lanes + layout)
     g = gpu_simulate(m, 3, 1 / 60, 15, (0.0, -9.8, 0.0), True, 0.9, lanes=lanes, layout=layout)
@@ -70,7 +70,7 @@ def test_prefetch_pdl_block_variants(gpu_device, prefetch, pdl, block):
     np.testing.assert_array_equal(g["x"], d["x"])
 
 
-@pytest.mark.parametrize("lanes,layout", [(4, 0), (8, 1), (16, 1), (32, 0)])
+@pytest.mark.parametrize("lanes,layout", [(4, 0), (8, 1), (16, 1), (32, 0), (8, 2), (4, 2)])
 @pytest.mark.parametrize("accel,substeps", [(True, 1), (False, 2)])
 def test_persistent_kernel_bit_identical(gpu_device, lanes, layout, accel, substeps):
     m = small_block(seed=lanes + layout, dims=(9, 5, 4), per_tet_sigma=0.2)
@@ -83,13 +83,27 @@ def test_persistent_kernel_bit_identical(gpu_device, lanes, layout, accel, subst
     assert b["launches"] == 4 * substeps  # one cooperative launch per sub-step
 
 
-def test_persistent_cube_matches_graph_path(gpu_device):
+@pytest.mark.parametrize("layout", [1, 2])
+def test_persistent_cube_matches_graph_path(gpu_device, layout):
     m = meshgen.cube(24)
     s = meshgen.CUBE_SETTINGS
-    a = gpu_simulate(m, 3, s["dt"], s["iterations"], s["gravity"], True, s["rho"], lanes=8, layout=1)
-    b = gpu_simulate(m, 3, s["dt"], s["iterations"], s["gravity"], True, s["rho"], lanes=8, layout=1,
+    a = gpu_simulate(m, 3, s["dt"], s["iterations"], s["gravity"], True, s["rho"], lanes=8, layout=layout)
+    b = gpu_simulate(m, 3, s["dt"], s["iterations"], s["gravity"], True, s["rho"], lanes=8, layout=layout,
                      options={_capi.OPT_PERSISTENT: 1})
     np.testing.assert_array_equal(a["x"], b["x"])
+
+
+@pytest.mark.parametrize("layout", [0, 1, 2])
+def test_layouts_on_reference_fixtures(gpu_device, layout):
+    """GPU vs the reference's own code (fixtures from its sources, tests/golden/make_ref_golden.py)."""
+    g = np.load(os.path.join(GOLDEN, "ref_trajectories.npz"))
+    m = meshgen.cube(6, seed=5)
+    st = meshgen.CUBE_SETTINGS
+    for steps in (1, 10):
+        r = gpu_simulate(m, steps, 1 / 120, 50, (0.0, -9.8, 0.0), True, 0.9, layout=layout)
+        err = rel_err(r["x"], g[f"cube6_stiff/x_s{steps}"], m)
+        print(f"cube6 layout {layout} {steps} steps vs reference: {err:.3e}")
+        assert err < POS_TOL
 
 
 @pytest.mark.parametrize("graph", [0, 1])

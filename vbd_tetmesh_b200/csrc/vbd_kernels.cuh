@@ -40,6 +40,8 @@ struct SweepParams {
     const int* inc_tet;
     const TetRec* rec;
     const TetRec* irec;
+    const int4* crec;          // compact incidence records, 3 x int4 per incidence (layout 2)
+    const float2* cmat;        // (V0 mu, V0 lambda) per incidence (layout 2)
     unsigned long long* status;
     int v_begin, v_end;
     float dtsr;                // 1/h^2
@@ -172,6 +174,101 @@ __device__ __forceinline__ void tet_contrib(const TetRec& r, int v, float4 xi, c
     }
 }
 
+// Compact incidence record (layout 2), 48 B + 8 B per (vertex, tet) incidence:
+//   int4  {nb0 | n << 30, nb1, nb2, q0.x}   the tet's other three vertices in local order, the
+//   float4{q0.y, q0.z, q1.x, q1.y}           vertex's own local index n, and rows q_k of
+//   float4{q1.z, q2.x, q2.y, q2.z}           Q = Ps Dm^-1 for those three vertices
+//   float2{V0 mu, V0 lambda}                 (separate stream)
+// Because the rows of Q sum to zero, F = Ds Dm^-1 = sum_k (x_k - x_n) q_k^T over the three other
+// vertices, and the vertex's own row is q_n = -(q0 + q1 + q2).
+struct CompactRec {
+    int nb0, nb1, nb2;
+    float q[9];
+    float a, b;  // V0 mu, V0 lambda
+};
+
+constexpr int kCompactIdMask = 0x3fffffff;
+
+__device__ __forceinline__ CompactRec load_compact(const int4* __restrict__ crec, const float2* __restrict__ cmat,
+                                                   int j) {
+    const int4 w0 = __ldg(crec + 3 * j);
+    const int4 w1 = __ldg(crec + 3 * j + 1);
+    const int4 w2 = __ldg(crec + 3 * j + 2);
+    const float2 m = __ldg(cmat + j);
+    CompactRec r;
+    r.nb0 = w0.x & kCompactIdMask;
+    r.nb1 = w0.y;
+    r.nb2 = w0.z;
+    r.q[0] = __int_as_float(w0.w);
+    r.q[1] = __int_as_float(w1.x);
+    r.q[2] = __int_as_float(w1.y);
+    r.q[3] = __int_as_float(w1.z);
+    r.q[4] = __int_as_float(w1.w);
+    r.q[5] = __int_as_float(w2.x);
+    r.q[6] = __int_as_float(w2.y);
+    r.q[7] = __int_as_float(w2.z);
+    r.q[8] = __int_as_float(w2.w);
+    r.a = m.x;
+    r.b = m.y;
+    return r;
+}
+
+// Same element block as tet_contrib, from a compact record: g_n = V P q_n,
+// H_nn = V (mu |q_n|^2 I + lambda (C q_n)(C q_n)^T), with V mu and V lambda premultiplied.
+template <bool WANT_H, bool COHERENT = false>
+__device__ __forceinline__ void compact_contrib(const CompactRec& r, float4 xi, const float4* __restrict__ X,
+                                                Acc& acc) {
+    const float4 p0 = load_pos<COHERENT>(X, r.nb0);
+    const float4 p1 = load_pos<COHERENT>(X, r.nb1);
+    const float4 p2 = load_pos<COHERENT>(X, r.nb2);
+    const float d0x = p0.x - xi.x, d0y = p0.y - xi.y, d0z = p0.z - xi.z;
+    const float d1x = p1.x - xi.x, d1y = p1.y - xi.y, d1z = p1.z - xi.z;
+    const float d2x = p2.x - xi.x, d2y = p2.y - xi.y, d2z = p2.z - xi.z;
+    const float* q = r.q;
+    const float F00 = d0x * q[0] + d1x * q[3] + d2x * q[6];
+    const float F01 = d0x * q[1] + d1x * q[4] + d2x * q[7];
+    const float F02 = d0x * q[2] + d1x * q[5] + d2x * q[8];
+    const float F10 = d0y * q[0] + d1y * q[3] + d2y * q[6];
+    const float F11 = d0y * q[1] + d1y * q[4] + d2y * q[7];
+    const float F12 = d0y * q[2] + d1y * q[5] + d2y * q[8];
+    const float F20 = d0z * q[0] + d1z * q[3] + d2z * q[6];
+    const float F21 = d0z * q[1] + d1z * q[4] + d2z * q[7];
+    const float F22 = d0z * q[2] + d1z * q[5] + d2z * q[8];
+    const float C00 = F11 * F22 - F12 * F21;
+    const float C01 = F12 * F20 - F10 * F22;
+    const float C02 = F10 * F21 - F11 * F20;
+    const float C10 = F21 * F02 - F22 * F01;
+    const float C11 = F22 * F00 - F20 * F02;
+    const float C12 = F20 * F01 - F21 * F00;
+    const float C20 = F01 * F12 - F02 * F11;
+    const float C21 = F02 * F10 - F00 * F12;
+    const float C22 = F00 * F11 - F01 * F10;
+    const float J = F00 * C00 + F01 * C01 + F02 * C02;
+    const float qx = -(q[0] + q[3] + q[6]);
+    const float qy = -(q[1] + q[4] + q[7]);
+    const float qz = -(q[2] + q[5] + q[8]);
+    const float Fq0 = F00 * qx + F01 * qy + F02 * qz;
+    const float Fq1 = F10 * qx + F11 * qy + F12 * qz;
+    const float Fq2 = F20 * qx + F21 * qy + F22 * qz;
+    const float Cq0 = C00 * qx + C01 * qy + C02 * qz;
+    const float Cq1 = C10 * qx + C11 * qy + C12 * qz;
+    const float Cq2 = C20 * qx + C21 * qy + C22 * qz;
+    const float bj = r.b * (J - 1.0f);
+    acc.g0 += r.a * (Fq0 - Cq0) + bj * Cq0;
+    acc.g1 += r.a * (Fq1 - Cq1) + bj * Cq1;
+    acc.g2 += r.a * (Fq2 - Cq2) + bj * Cq2;
+    if (WANT_H) {
+        const float am = r.a * (qx * qx + qy * qy + qz * qz);
+        const float b0 = r.b * Cq0, b1 = r.b * Cq1, b2 = r.b * Cq2;
+        acc.h00 += am + b0 * Cq0;
+        acc.h01 += b0 * Cq1;
+        acc.h02 += b0 * Cq2;
+        acc.h11 += am + b1 * Cq1;
+        acc.h12 += b1 * Cq2;
+        acc.h22 += am + b2 * Cq2;
+    }
+}
+
 template <int LANES>
 __device__ __forceinline__ void group_reduce(Acc& a) {
 #pragma unroll
@@ -188,10 +285,36 @@ __device__ __forceinline__ void group_reduce(Acc& a) {
     }
 }
 
-template <bool STREAM>
-__device__ __forceinline__ TetRec fetch_rec(const SweepParams& p, int j) {
-    return STREAM ? load_rec(p.irec + j) : load_rec(p.rec + __ldg(p.inc_tet + j));
-}
+// Element data of incidence j under each record layout:
+//   0 = tet record gathered through inc_tet, 1 = tet record streamed in incidence order,
+//   2 = compact streamed record.
+template <int LAYOUT> struct Elem;
+template <> struct Elem<0> {
+    using Rec = TetRec;
+    __device__ __forceinline__ static Rec fetch(const SweepParams& p, int j) {
+        return load_rec(p.rec + __ldg(p.inc_tet + j));
+    }
+    template <bool COHERENT>
+    __device__ __forceinline__ static void contrib(const Rec& r, int v, float4 xi, const float4* X, Acc& acc) {
+        tet_contrib<true, COHERENT>(r, v, xi, X, acc);
+    }
+};
+template <> struct Elem<1> {
+    using Rec = TetRec;
+    __device__ __forceinline__ static Rec fetch(const SweepParams& p, int j) { return load_rec(p.irec + j); }
+    template <bool COHERENT>
+    __device__ __forceinline__ static void contrib(const Rec& r, int v, float4 xi, const float4* X, Acc& acc) {
+        tet_contrib<true, COHERENT>(r, v, xi, X, acc);
+    }
+};
+template <> struct Elem<2> {
+    using Rec = CompactRec;
+    __device__ __forceinline__ static Rec fetch(const SweepParams& p, int j) { return load_compact(p.crec, p.cmat, j); }
+    template <bool COHERENT>
+    __device__ __forceinline__ static void contrib(const Rec& r, int, float4 xi, const float4* X, Acc& acc) {
+        compact_contrib<true, COHERENT>(r, xi, X, acc);
+    }
+};
 
 // The vertex block update of VBDsolver::solveVertex + solve (VBD.cpp:124-203) for vertex v:
 // LANES threads split its incident tets, reduce with warp shuffles, and the group's first lane
@@ -199,25 +322,25 @@ __device__ __forceinline__ TetRec fetch_rec(const SweepParams& p, int j) {
 // |det| > 1e-8 guard (VBD.cpp:141-152, Types.h:85-112), then writes x~, the Chebyshev blend
 // x^(k) = omega (x~ - pp) + pp (VBD.cpp:290-300) and the pre-sweep position into pp.
 // Every lane of the warp must call it (shuffles); `active` marks lanes with a real vertex.
-//   STREAM   : element records read from the incidence-ordered copy instead of through inc_tet
+//   LAYOUT   : element record layout (Elem<0/1/2>)
 //   PREFETCH : the next element record is loaded while the current one is evaluated
 //   COHERENT : positions read with coherent loads (persistent kernel)
 // `nxt` holds the lane's first record if PREFETCH (fetched by the caller).
-template <int LANES, bool STREAM, bool PREFETCH, bool COHERENT>
+template <int LANES, int LAYOUT, bool PREFETCH, bool COHERENT>
 __device__ __forceinline__ void vertex_update(const SweepParams& p, int v, int lane, bool active, int j, int j1,
-                                              TetRec nxt) {
+                                              typename Elem<LAYOUT>::Rec nxt) {
     const float4 xi = active ? p.x[v] : make_float4(0.f, 0.f, 0.f, 0.f);
     Acc acc;
     acc.zero();
     for (; j < j1; j += LANES) {
-        TetRec r;
+        typename Elem<LAYOUT>::Rec r;
         if (PREFETCH) {
             r = nxt;
-            if (j + LANES < j1) nxt = fetch_rec<STREAM>(p, j + LANES);
+            if (j + LANES < j1) nxt = Elem<LAYOUT>::fetch(p, j + LANES);
         } else {
-            r = fetch_rec<STREAM>(p, j);
+            r = Elem<LAYOUT>::fetch(p, j);
         }
-        tet_contrib<true, COHERENT>(r, v, xi, p.x, acc);
+        Elem<LAYOUT>::template contrib<COHERENT>(r, v, xi, p.x, acc);
     }
     group_reduce<LANES>(acc);
     if (!active || lane != 0) return;
@@ -263,7 +386,7 @@ __device__ __forceinline__ void vertex_update(const SweepParams& p, int v, int l
 // One colour of one Gauss-Seidel sweep per launch (VBDsolver::solve, VBD.cpp:114-158).  Element
 // data never changes during a sweep, so the lane's first record is fetched before the dependency
 // wait; positions are read only after it.
-template <int LANES, bool STREAM, bool PREFETCH>
+template <int LANES, int LAYOUT, bool PREFETCH>
 __global__ void __launch_bounds__(256) k_sweep(SweepParams p) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = LANES == 1 ? 0 : (threadIdx.x & (LANES - 1));
@@ -275,11 +398,11 @@ __global__ void __launch_bounds__(256) k_sweep(SweepParams p) {
         j1 = __ldg(p.inc_off + v + 1);
     }
     const int j = j0 + lane;
-    TetRec nxt;
-    if (PREFETCH && j < j1) nxt = fetch_rec<STREAM>(p, j);
+    typename Elem<LAYOUT>::Rec nxt;
+    if (PREFETCH && j < j1) nxt = Elem<LAYOUT>::fetch(p, j);
     pdl_trigger();
     pdl_wait();
-    vertex_update<LANES, STREAM, PREFETCH, false>(p, v, lane, active, j, j1, nxt);
+    vertex_update<LANES, LAYOUT, PREFETCH, false>(p, v, lane, active, j, j1, nxt);
 }
 
 // ---- persistent colour-walking kernel -------------------------------------------------------
@@ -354,7 +477,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, int expected, lon
 // Whole step (or solve) in one cooperative launch: predictor, `iters` sweeps over the colours
 // with a grid barrier after each colour, velocity update.  Same arithmetic as k_predict /
 // k_sweep / k_finish, so results are bit-identical to the multi-launch path.
-template <int LANES, bool STREAM>
+template <int LANES, int LAYOUT>
 __global__ void __launch_bounds__(256, 4) k_persistent(PersistParams p) {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nthreads = gridDim.x * blockDim.x;
@@ -418,9 +541,9 @@ __global__ void __launch_bounds__(256, 4) k_persistent(PersistParams p) {
                     j1 = __ldg(sp.inc_off + v + 1);
                 }
                 const int j = j0 + lane;
-                TetRec nxt;
-                if (j < j1) nxt = fetch_rec<STREAM>(sp, j);
-                vertex_update<LANES, STREAM, true, true>(sp, v, lane, active, j, j1, nxt);
+                typename Elem<LAYOUT>::Rec nxt;
+                if (j < j1) nxt = Elem<LAYOUT>::fetch(sp, j);
+                vertex_update<LANES, LAYOUT, true, true>(sp, v, lane, active, j, j1, nxt);
             }
             if (!grid_barrier(p.bar, p.expected_blocks, p.spin_limit, p.sw.status)) return;
         }
@@ -544,6 +667,44 @@ __global__ void k_pack_stream(const TetRec* __restrict__ rec, const int* __restr
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ninc) return;
     irec[j] = rec[inc_tet[j]];
+}
+
+// Compact incidence records from the tet records (layout 2): for incidence j of vertex v (internal
+// id, inc_vertex[j]) in tet inc_tet[j], the other three vertices in local order with their rows
+// of Q = Ps Dm^-1, the vertex's local index, and (V0 mu, V0 lambda).
+__global__ void k_pack_compact(const TetRec* __restrict__ rec, const int* __restrict__ inc_tet,
+                               const int* __restrict__ inc_vertex, int4* __restrict__ crec, float2* __restrict__ cmat,
+                               int ninc) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ninc) return;
+    const TetRec r = rec[inc_tet[j]];
+    const int v = inc_vertex[j];
+    const int ids[4] = {r.ids.x, r.ids.y, r.ids.z, r.ids.w};
+    const float D[3][3] = {{r.a.x, r.a.y, r.a.z}, {r.a.w, r.b.x, r.b.y}, {r.b.z, r.b.w, r.c.x}};
+    float Q[4][3];
+    for (int c = 0; c < 3; ++c) {
+        Q[0][c] = -D[0][c] - D[1][c] - D[2][c];
+        for (int k = 1; k < 4; ++k) Q[k][c] = D[k - 1][c];
+    }
+    int n = 3;
+    for (int k = 0; k < 4; ++k)
+        if (ids[k] == v) {
+            n = k;
+            break;
+        }
+    int nb[3];
+    float q[9];
+    int m = 0;
+    for (int k = 0; k < 4; ++k) {
+        if (k == n) continue;
+        nb[m] = ids[k];
+        for (int c = 0; c < 3; ++c) q[3 * m + c] = Q[k][c];
+        ++m;
+    }
+    crec[3 * j] = make_int4(nb[0] | (n << 30), nb[1], nb[2], __float_as_int(q[0]));
+    crec[3 * j + 1] = make_int4(__float_as_int(q[1]), __float_as_int(q[2]), __float_as_int(q[3]), __float_as_int(q[4]));
+    crec[3 * j + 2] = make_int4(__float_as_int(q[5]), __float_as_int(q[6]), __float_as_int(q[7]), __float_as_int(q[8]));
+    cmat[j] = make_float2(r.c.y * r.c.z, r.c.y * r.c.w);
 }
 
 // ---- FP64 reductions (energies, residual) ---------------------------------------------------

@@ -60,19 +60,22 @@ static float omega_of(int order, float rho, float prev) {
 
 using SweepFn = void (*)(SweepParams);
 
-template <int L> static SweepFn pick_sweep(bool stream, bool prefetch) {
-    if (stream) return prefetch ? &k_sweep<L, true, true> : &k_sweep<L, true, false>;
-    return prefetch ? &k_sweep<L, false, true> : &k_sweep<L, false, false>;
+template <int L> static SweepFn pick_sweep(int layout, bool prefetch) {
+    switch (layout) {
+        case 0: return prefetch ? &k_sweep<L, 0, true> : &k_sweep<L, 0, false>;
+        case 1: return prefetch ? &k_sweep<L, 1, true> : &k_sweep<L, 1, false>;
+        default: return prefetch ? &k_sweep<L, 2, true> : &k_sweep<L, 2, false>;
+    }
 }
 
-static SweepFn pick_sweep(int lanes, bool stream, bool prefetch) {
+static SweepFn pick_sweep(int lanes, int layout, bool prefetch) {
     switch (lanes) {
-        case 1: return pick_sweep<1>(stream, prefetch);
-        case 2: return pick_sweep<2>(stream, prefetch);
-        case 4: return pick_sweep<4>(stream, prefetch);
-        case 8: return pick_sweep<8>(stream, prefetch);
-        case 16: return pick_sweep<16>(stream, prefetch);
-        default: return pick_sweep<32>(stream, prefetch);
+        case 1: return pick_sweep<1>(layout, prefetch);
+        case 2: return pick_sweep<2>(layout, prefetch);
+        case 4: return pick_sweep<4>(layout, prefetch);
+        case 8: return pick_sweep<8>(layout, prefetch);
+        case 16: return pick_sweep<16>(layout, prefetch);
+        default: return pick_sweep<32>(layout, prefetch);
     }
 }
 
@@ -104,12 +107,15 @@ struct vbd_solver {
     vbd::DBuf<float4> x0, x1, pp, y, v, xprev;
     vbd::DBuf<int> perm, inc_off, inc_tet;
     vbd::DBuf<vbd::TetRec> rec, irec;
+    vbd::DBuf<int4> crec;                           // compact incidence records (layout 2)
+    vbd::DBuf<float2> cmat;
+    vbd::DBuf<int> inc_vertex;                      // internal vertex of each incidence
     vbd::DBuf<float> stage, mat_stage;
     vbd::DBuf<unsigned long long> status;
     vbd::DBuf<double> partials, scalar;
-    // defaults: the fastest shape measured on the 64^3 cube (streamed records, 8 lanes per vertex,
-    // record prefetch, programmatic dependent launch, 128-thread blocks)
-    int lanes = 8, layout = 1, use_graph = 1, timing = 0, prefetch = 1, pdl = 1, block = 128;
+    // defaults: the fastest shape measured on the 64^3 cube (compact streamed records, 4 lanes per
+    // vertex, record prefetch, programmatic dependent launch, 128-thread blocks)
+    int lanes = 4, layout = 2, use_graph = 1, timing = 0, prefetch = 1, pdl = 1, block = 128;
     int persistent = 0;                             // whole step in one cooperative launch
     long long spin_limit = 1LL << 22;               // barrier polls before a persistent launch gives up
     vbd::DBuf<int> d_cstart;
@@ -179,10 +185,11 @@ struct vbd_solver {
     int launch_sweep(int c, float4* xr, float4* xn, bool accel, bool keep_pp, float dtsr, float omega) {
         const int vb = cstart[c], ve = cstart[c + 1];
         if (ve <= vb) return VBD_OK;
-        vbd::SweepParams p{xr,   xn, pp.p, y.p,   inc_off.p,     inc_tet.p,         rec.p,
-                           irec.p, status.p, vb, ve, dtsr, omega, accel ? 1 : 0, keep_pp ? 1 : 0};
+        vbd::SweepParams p{xr,     xn,     pp.p,     y.p, inc_off.p, inc_tet.p, rec.p,          irec.p,
+                           crec.p, cmat.p, status.p, vb,  ve,        dtsr,      omega, accel ? 1 : 0,
+                           keep_pp ? 1 : 0};
         const long long threads = (long long)(ve - vb) * lanes;
-        vbd::SweepFn fn = vbd::pick_sweep(lanes, layout == 1, prefetch != 0);
+        vbd::SweepFn fn = vbd::pick_sweep(lanes, layout, prefetch != 0);
         cudaEvent_t ev[2] = {nullptr, nullptr};
         if (timing) {
             VBD_TRY(timing_event(ev));
@@ -280,12 +287,19 @@ struct vbd_solver {
         }
         const int L = lanes < 4 ? 4 : lanes;
         void (*fn)(vbd::PersistParams) = nullptr;
-        const bool st = layout == 1;
-        switch (L) {
-            case 4: fn = st ? &vbd::k_persistent<4, true> : &vbd::k_persistent<4, false>; break;
-            case 8: fn = st ? &vbd::k_persistent<8, true> : &vbd::k_persistent<8, false>; break;
-            case 16: fn = st ? &vbd::k_persistent<16, true> : &vbd::k_persistent<16, false>; break;
-            default: fn = st ? &vbd::k_persistent<32, true> : &vbd::k_persistent<32, false>; break;
+        switch (L * 4 + layout) {
+            case 16: fn = &vbd::k_persistent<4, 0>; break;
+            case 17: fn = &vbd::k_persistent<4, 1>; break;
+            case 18: fn = &vbd::k_persistent<4, 2>; break;
+            case 32: fn = &vbd::k_persistent<8, 0>; break;
+            case 33: fn = &vbd::k_persistent<8, 1>; break;
+            case 34: fn = &vbd::k_persistent<8, 2>; break;
+            case 64: fn = &vbd::k_persistent<16, 0>; break;
+            case 65: fn = &vbd::k_persistent<16, 1>; break;
+            case 66: fn = &vbd::k_persistent<16, 2>; break;
+            case 128: fn = &vbd::k_persistent<32, 0>; break;
+            case 129: fn = &vbd::k_persistent<32, 1>; break;
+            default: fn = &vbd::k_persistent<32, 2>; break;
         }
         int per_sm = 0, sms = 0;
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0));
@@ -293,8 +307,8 @@ struct vbd_solver {
         if (per_sm < 1) VBD_FAIL(VBD_ERR_CUDA, "persistent kernel cannot be resident");
         const int grid = per_sm * sms;
         vbd::PersistParams pp_{};
-        pp_.sw = vbd::SweepParams{x0.p, x1.p, pp.p,   y.p,  inc_off.p, inc_tet.p, rec.p, irec.p,
-                                  status.p, 0, 0,     dtsr, 1.0f, 0, accel ? 1 : 0};
+        pp_.sw = vbd::SweepParams{x0.p, x1.p, pp.p, y.p,  inc_off.p, inc_tet.p, rec.p, irec.p, crec.p, cmat.p,
+                                  status.p, 0,  0,    dtsr, 1.0f,      0,         accel ? 1 : 0};
         pp_.xa = x0.p;
         pp_.xb = x1.p;
         pp_.v = v.p;
@@ -377,22 +391,37 @@ struct vbd_solver {
     }
 
     // Captured graphs bake in buffer addresses: every (re)allocation or release of the streamed
-    // record copy invalidates them.
+    // record copies invalidates them.
     int repack_stream() {
-        if (layout != 1) {
-            if (irec.p) {
-                drop_graphs();
-                irec.release();
-            }
-            return VBD_OK;
-        }
-        if (irec.n != (size_t)ninc) {
+        if (layout != 1 && irec.p) {
             drop_graphs();
-            VBD_TRY(irec.alloc(ninc));
+            irec.release();
         }
-        if (ninc > 0) {
-            vbd::k_pack_stream<<<vbd::nblk(ninc, 256), 256, 0, stream>>>(rec.p, inc_tet.p, irec.p, (int)ninc);
-            VBD_TRY(check_launch());
+        if (layout != 2 && crec.p) {
+            drop_graphs();
+            crec.release();
+            cmat.release();
+        }
+        if (layout == 1) {
+            if (irec.n != (size_t)ninc) {
+                drop_graphs();
+                VBD_TRY(irec.alloc(ninc));
+            }
+            if (ninc > 0) {
+                vbd::k_pack_stream<<<vbd::nblk(ninc, 256), 256, 0, stream>>>(rec.p, inc_tet.p, irec.p, (int)ninc);
+                VBD_TRY(check_launch());
+            }
+        } else if (layout == 2) {
+            if (crec.n != 3 * (size_t)ninc) {
+                drop_graphs();
+                VBD_TRY(crec.alloc(3 * (size_t)ninc));
+                VBD_TRY(cmat.alloc(ninc));
+            }
+            if (ninc > 0) {
+                vbd::k_pack_compact<<<vbd::nblk(ninc, 256), 256, 0, stream>>>(rec.p, inc_tet.p, inc_vertex.p, crec.p,
+                                                                             cmat.p, (int)ninc);
+                VBD_TRY(check_launch());
+            }
         }
         return VBD_OK;
     }
@@ -515,6 +544,9 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->ready = false;
     s->drop_graphs();
+    s->irec.release();
+    s->crec.release();
+    s->cmat.release();
 
     // Internal order: free vertices colour by colour (group order), then the pinned ones.
     std::vector<int32_t> perm;
@@ -539,9 +571,11 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     for (int i = 0; i < nfree; ++i) inc_off[i + 1] = inc_off[i] + (voff[perm[i] + 1] - voff[perm[i]]);
     for (int i = nfree; i < N; ++i) inc_off[i + 1] = inc_off[i];
     const long long ninc = inc_off[N];
-    std::vector<int32_t> inc_tet(std::max<long long>(ninc, 1));
-    for (int i = 0; i < nfree; ++i)
+    std::vector<int32_t> inc_tet(std::max<long long>(ninc, 1)), inc_vertex(std::max<long long>(ninc, 1));
+    for (int i = 0; i < nfree; ++i) {
         std::copy(vtets.begin() + voff[perm[i]], vtets.begin() + voff[perm[i] + 1], inc_tet.begin() + inc_off[i]);
+        std::fill(inc_vertex.begin() + inc_off[i], inc_vertex.begin() + inc_off[i + 1], i);
+    }
 
     std::vector<vbd::TetRec> rec(std::max(T, 1));
     for (int t = 0; t < T; ++t) {
@@ -573,6 +607,7 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     VBD_TRY(s->perm.alloc(N));
     VBD_TRY(s->inc_off.alloc(N + 1));
     VBD_TRY(s->inc_tet.alloc(inc_tet.size()));
+    VBD_TRY(s->inc_vertex.alloc(inc_vertex.size()));
     VBD_TRY(s->rec.alloc(rec.size()));
     VBD_TRY(s->stage.alloc(3LL * N));
     VBD_TRY(s->mat_stage.alloc(2LL * std::max(T, 1)));
@@ -588,6 +623,7 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     CUDA_TRY(cudaMemcpy(s->perm.p, perm.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->inc_off.p, inc_off.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->inc_tet.p, inc_tet.data(), sizeof(int) * inc_tet.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->inc_vertex.p, inc_vertex.data(), sizeof(int) * inc_vertex.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->rec.p, rec.data(), sizeof(vbd::TetRec) * rec.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemset(s->status.p, 0, sizeof(unsigned long long) * vbd::ST_SLOTS));
 
@@ -828,8 +864,9 @@ int vbd_solver_energy(vbd_solver* s, int32_t kind, float h, double* out) {
             *out = 0.0;
             return VBD_OK;
         }
-        vbd::SweepParams p{s->x0.p, nullptr, s->pp.p, s->y.p, s->inc_off.p, s->inc_tet.p, s->rec.p, s->irec.p,
-                           s->status.p, 0, s->nfree, (float)(1.0 / ((double)h * h)), 1.0f};
+        vbd::SweepParams p{s->x0.p,     nullptr, s->pp.p,    s->y.p, s->inc_off.p, s->inc_tet.p,
+                           s->rec.p,    s->irec.p, s->crec.p, s->cmat.p, s->status.p, 0,
+                           s->nfree,    (float)(1.0 / ((double)h * h)), 1.0f};
         const int L = std::max(4, s->lanes);
         const unsigned blocks = vbd::nblk((long long)s->nfree * L, 256);
         switch (L) {
@@ -894,7 +931,7 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
             s->block = value;
             return VBD_OK;
         case VBD_OPT_LAYOUT:
-            if (value != 0 && value != 1) VBD_FAIL(VBD_ERR_INVALID_ARG, "layout must be 0 or 1");
+            if (value < 0 || value > 2) VBD_FAIL(VBD_ERR_INVALID_ARG, "layout must be 0, 1 or 2");
             s->layout = value;
             if (s->ready) {
                 VBD_TRY(s->repack_stream());
@@ -976,9 +1013,9 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
         int lanes, layout, prefetch, pdl, block;
     };
     static const Cand cands[] = {
-        {8, 1, 1, 1, 128}, {4, 1, 1, 1, 128}, {8, 1, 1, 0, 128}, {4, 1, 1, 0, 128}, {16, 1, 1, 1, 128},
-        {2, 1, 1, 0, 128}, {8, 0, 1, 1, 128}, {4, 0, 1, 1, 128}, {8, 0, 1, 0, 128}, {4, 0, 1, 0, 128},
-        {8, 1, 1, 1, 256}, {4, 1, 1, 1, 256},
+        {4, 2, 1, 1, 128}, {8, 2, 1, 1, 128}, {8, 2, 0, 1, 128}, {2, 2, 1, 1, 128}, {16, 2, 1, 1, 128},
+        {4, 2, 1, 0, 128}, {4, 2, 1, 1, 256}, {8, 1, 1, 1, 128}, {4, 1, 1, 1, 128}, {8, 0, 1, 1, 128},
+        {4, 0, 1, 1, 128}, {8, 0, 1, 0, 128},
     };
     const float g[3] = {0.f, 0.f, 0.f};
     cudaEvent_t e0, e1;
