@@ -1,0 +1,229 @@
+// VBD.h -- VBDParams and VBDsolver with the reference's API (VBD.h:14-140), running on the GPU.
+//
+// step() / simulate() keep the reference's semantics (VBDsolver::step, VBD.cpp:60-101: predictor,
+// numIterations Gauss-Seidel colour sweeps with the Chebyshev blend, velocity update x 0.999) but
+// execute through libvbd_b200: the TetMesh's positions and velocities are uploaded, one
+// vbd_solver_step runs on the device, and positions, velocities and the inertial target are read
+// back.  Colouring and Dm^-1 / V0 are computed by the library bit-exactly with the reference.
+// Differences from the reference, by design:
+//   * numThreads is ignored (the GPU sweeps each colour in parallel; results equal the reference's
+//     single-thread run up to summation order, without its colour-loop race, VBD.cpp:120);
+//   * energyHistory gets one computeTotalEnergy value per step when recordEnergyHistory is set
+//     (the reference evaluates it every 10th iteration inside step);
+//   * solveVertex / computeTetContribution (per-vertex CPU helpers) are not provided.
+#pragma once
+
+#include <functional>
+#include <vector>
+
+#include "GraphColoring.h"
+#include "TetMesh.h"
+#include "Types.h"
+
+namespace VBD {
+
+struct VBDParams {
+    Real dt = 0.01666666f;
+    int numIterations = 50;
+    int substeps = 1;
+    Vec3 gravity{0, -9.8f, 0};
+    bool useAcceleration = false;
+    Real accelerationRho = 0.75f;
+    int numThreads = 4;  // accepted for compatibility; the sweep runs on the GPU
+    Real mu = 1e6f;
+    Real lambda = 1e6f;
+    Real density = 1000.0f;
+    // extensions
+    bool usePerTetMaterials = false;   // use TetMesh::tetMu / tetLambda instead of mu / lambda
+    bool recordEnergyHistory = false;  // push computeTotalEnergy after every step
+    int device = 0;                    // CUDA device of the solver
+};
+
+class VBDsolver {
+  public:
+    VBDsolver() = default;
+    ~VBDsolver() { release(); }
+    VBDsolver(const VBDsolver&) = delete;
+    VBDsolver& operator=(const VBDsolver&) = delete;
+
+    void setParams(const VBDParams& p) { params = p; }
+
+    void initializeColoring(const TetMesh& mesh) {
+        vertexColors = GraphColoring::colorVertices(mesh.vertAdjacentTets, mesh.tets, mesh.numVerts);
+        prevPrevPos.resize(3, (Eigen::Index)mesh.numVerts);
+        prevPrevPos.setZero();
+    }
+
+    void precomputeTetData(const TetMesh& mesh) {
+        const std::vector<int32_t> flat = flatTets(mesh);
+        std::vector<float> dm(9 * mesh.numTets);
+        tetRestVolume.assign(mesh.numTets, 0.0f);
+        vbdCheck(vbd_precompute_tets((int32_t)mesh.numVerts, (int32_t)mesh.numTets, mesh.mRestPos.data(), flat.data(),
+                                     dm.data(), tetRestVolume.data()),
+                 "vbd_precompute_tets");
+        tetDmInv.assign(mesh.numTets, Matrix3r());
+        for (size_t t = 0; t < mesh.numTets; ++t)
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) tetDmInv[t](a, b) = dm[9 * t + 3 * a + b];
+    }
+
+    void step(TetMesh& mesh) {
+        if (vertexColors.empty()) {
+            initializeColoring(mesh);
+            precomputeTetData(mesh);
+        }
+        ensureDevice(mesh);
+        vbdCheck(vbd_solver_set_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_set_positions");
+        vbdCheck(vbd_solver_set_velocities(gpu_, mesh.mVelocity.data()), "vbd_solver_set_velocities");
+        mesh.savePreviousPosition();
+        const float g[3] = {params.gravity[0], params.gravity[1], params.gravity[2]};
+        vbdCheck(vbd_solver_step(gpu_, params.dt, params.substeps, params.numIterations, g,
+                                 params.useAcceleration ? 1 : 0, params.accelerationRho),
+                 "vbd_solver_step");
+        vbdCheck(vbd_solver_get_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_get_positions");
+        vbdCheck(vbd_solver_get_velocities(gpu_, mesh.mVelocity.data()), "vbd_solver_get_velocities");
+        vbdCheck(vbd_solver_get_inertia(gpu_, mesh.mInertia.data()), "vbd_solver_get_inertia");
+        if (params.recordEnergyHistory) energyHistory.push_back(computeTotalEnergy(mesh));
+    }
+
+    void simulate(TetMesh& mesh, int numFrames, std::function<void(int, TetMesh&)> callback = nullptr) {
+        energyHistory.clear();
+        for (int frame = 0; frame < numFrames; ++frame) {
+            step(mesh);
+            if (callback) callback(frame, mesh);
+        }
+    }
+
+    // Elastic log-J Neo-Hookean energy of the mesh's current positions (VBD.cpp:258-288), summed
+    // in FP64 on the device.
+    Real computeTotalEnergy(const TetMesh& mesh) const {
+        ensureDevice(mesh);
+        vbdCheck(vbd_solver_set_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_set_positions");
+        double e = 0.0;
+        vbdCheck(vbd_solver_energy(gpu_, VBD_ENERGY_ELASTIC_LOGJ, 1.0f, &e), "vbd_solver_energy");
+        return (Real)e;
+    }
+
+    const std::vector<std::vector<IdType>>& getVertexColors() const { return vertexColors; }
+    const std::vector<Matrix3r>& getTetDmInv() const { return tetDmInv; }
+    const std::vector<Real>& getTetRestVol() const { return tetRestVolume; }
+
+    VBDParams params;
+    std::vector<std::vector<IdType>> vertexColors;
+    TVerticesMat prevPrevPos;
+    std::vector<Real> energyHistory;
+    std::vector<Matrix3r> tetDmInv;
+    std::vector<Real> tetRestVolume;
+
+    // Predictor on the host, as the reference (VBD.cpp:103-112).
+    void forwardStep(TetMesh& mesh) {
+        mesh.savePreviousPosition();
+        mesh.applyGravity(params.gravity, params.dt / params.substeps);
+        mesh.computeInertia(params.dt / params.substeps);
+    }
+
+    // One Gauss-Seidel sweep over all colours from mesh.mVertPos towards mesh.mInertia
+    // (VBD.cpp:114-158), on the device.
+    void solve(TetMesh& mesh) {
+        if (vertexColors.empty()) {
+            initializeColoring(mesh);
+            precomputeTetData(mesh);
+        }
+        ensureDevice(mesh);
+        const Real dt = params.dt / params.substeps;
+        const Real dtsr = (Real)(1.0 / (dt * dt));
+        vbdCheck(vbd_solver_set_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_set_positions");
+        vbdCheck(vbd_solver_set_inertia(gpu_, mesh.mInertia.data()), "vbd_solver_set_inertia");
+        vbdCheck(vbd_solver_solve_iteration(gpu_, dtsr), "vbd_solver_solve_iteration");
+        vbdCheck(vbd_solver_get_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_get_positions");
+    }
+
+    // x = omega (x - x_pp) + x_pp on free vertices (VBD.cpp:290-300), on the host.
+    void applyAcceleration(TetMesh& mesh, Real omega) {
+        if (omega <= 1.0) return;
+        for (size_t i = 0; i < mesh.numVerts; ++i)
+            if (!mesh.isFixed[i])
+                for (int c = 0; c < 3; ++c) {
+                    const Eigen::Index k = (Eigen::Index)i;
+                    mesh.mVertPos(c, k) = omega * (mesh.mVertPos(c, k) - prevPrevPos(c, k)) + prevPrevPos(c, k);
+                }
+    }
+
+    // Chebyshev weights (VBD.cpp:302-311).
+    Real getAcceleratorOmega(int order, Real rho, Real prevOmega) {
+        if (order == 1) return 1.0f;
+        if (order == 2) return (Real)(2.0 / (2.0 - (double)(rho * rho)));
+        return (Real)(4.0 / (4.0 - (double)(rho * rho * prevOmega)));
+    }
+
+    // The C-ABI handle (null before the first step); for callers mixing both APIs.
+    vbd_solver* deviceHandle() const { return gpu_; }
+
+  private:
+    static std::vector<int32_t> flatTets(const TetMesh& mesh) {
+        std::vector<int32_t> flat(4 * mesh.numTets);
+        for (size_t t = 0; t < mesh.numTets; ++t)
+            for (int a = 0; a < 4; ++a) flat[4 * t + a] = mesh.tets[t][a];
+        return flat;
+    }
+
+    void ensureDevice(const TetMesh& mesh) const {
+        if (gpu_ && devVerts_ == mesh.numVerts && devTets_ == mesh.numTets) {
+            syncMaterials(mesh);
+            return;
+        }
+        if (!gpu_) vbdCheck(vbd_solver_create(&gpu_, params.device, nullptr), "vbd_solver_create");
+        const std::vector<int32_t> flat = flatTets(mesh);
+        std::vector<uint8_t> fixed(mesh.numVerts);
+        for (size_t i = 0; i < mesh.numVerts; ++i) fixed[i] = mesh.isFixed[i] ? 1 : 0;
+        std::vector<int32_t> offs(1, 0), verts;
+        for (const auto& g : vertexColors) {
+            verts.insert(verts.end(), g.begin(), g.end());
+            offs.push_back((int32_t)verts.size());
+        }
+        std::vector<float> dm(9 * mesh.numTets);
+        for (size_t t = 0; t < mesh.numTets; ++t)
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) dm[9 * t + 3 * a + b] = tetDmInv[t](a, b);
+        std::vector<float> mass(mesh.numVerts);
+        for (size_t i = 0; i < mesh.numVerts; ++i) mass[i] = mesh.vertexMass((Eigen::Index)i);
+        vbdCheck(vbd_solver_init(gpu_, (int32_t)mesh.numVerts, (int32_t)mesh.numTets, mesh.mVertPos.data(),
+                                 mesh.mVelocity.data(), mesh.mInertia.data(), mass.data(), fixed.data(), flat.data(),
+                                 (int32_t)vertexColors.size(), offs.data(), verts.data(), dm.data(),
+                                 tetRestVolume.data(), nullptr, nullptr),
+                 "vbd_solver_init");
+        devVerts_ = mesh.numVerts;
+        devTets_ = mesh.numTets;
+        matKey_.clear();
+        syncMaterials(mesh);
+    }
+
+    // Materials as the reference uses them: params.mu / lambda for every tet (VBD.cpp:214-215), or
+    // the mesh's per-tet values when usePerTetMaterials is set.
+    void syncMaterials(const TetMesh& mesh) const {
+        std::vector<float> key;
+        if (params.usePerTetMaterials) {
+            key = mesh.tetMu;
+            key.insert(key.end(), mesh.tetLambda.begin(), mesh.tetLambda.end());
+        } else {
+            key = {params.mu, params.lambda};
+        }
+        if (key == matKey_) return;
+        if (params.usePerTetMaterials)
+            vbdCheck(vbd_solver_set_materials(gpu_, mesh.tetMu.data(), mesh.tetLambda.data()), "vbd_solver_set_materials");
+        else
+            vbdCheck(vbd_solver_set_uniform_material(gpu_, params.mu, params.lambda), "vbd_solver_set_uniform_material");
+        matKey_ = key;
+    }
+
+    void release() {
+        if (gpu_) vbd_solver_destroy(gpu_);
+        gpu_ = nullptr;
+    }
+
+    mutable vbd_solver* gpu_ = nullptr;
+    mutable size_t devVerts_ = 0, devTets_ = 0;
+    mutable std::vector<float> matKey_;
+};
+
+}  // namespace VBD

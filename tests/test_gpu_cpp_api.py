@@ -1,0 +1,84 @@
+"""The C++ drop-in surface on the GPU: tests/cpp/test_cpp_api runs the reference's two calling
+patterns (VBDsolver::step, and the main.cpp loop over VBD_GPU_Solver) through include/vbd/*.h and
+libvbd_b200; results are checked against the oracle."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import rel_err
+from oracle import pyoracle as po
+from vbd_tetmesh_b200 import meshgen
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CPP_DIR = os.path.join(ROOT, "tests", "cpp")
+BIN = os.path.join(CPP_DIR, "test_cpp_api")
+
+
+def run_cpp(m, iters, steps, dt, rho, tmp_path):
+    if not os.path.exists(BIN):
+        subprocess.run(["make", "-C", CPP_DIR], check=True, capture_output=True)
+    inp = tmp_path / "in.bin"
+    with open(inp, "wb") as f:
+        np.array([m.num_verts, m.num_tets, iters, steps], np.int32).tofile(f)
+        np.array([m.density, m.mu[0], m.lam[0], dt, rho], np.float32).tofile(f)
+        m.rest.astype(np.float32).tofile(f)
+        m.tets.astype(np.int32).tofile(f)
+        m.fixed.astype(np.uint8).tofile(f)
+    out = tmp_path / "out.bin"
+    obj = tmp_path / "mesh.obj"
+    r = subprocess.run([BIN, str(inp), str(out), str(obj)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    raw = open(out, "rb").read()
+    n3 = 3 * m.num_verts
+    f = np.frombuffer(raw[: 4 * (3 * n3 + 1)], np.float32)
+    tail = np.frombuffer(raw[4 * (3 * n3 + 1):], np.int32)
+    return dict(x1=f[:n3].reshape(-1, 3), v1=f[n3:2 * n3].reshape(-1, 3), x2=f[2 * n3:3 * n3].reshape(-1, 3),
+                energy=float(f[3 * n3]), nsurf=int(tail[0]), ncol=int(tail[1]), obj=obj)
+
+
+def wrapper_flow_oracle(m, iters, steps, dt, rho):
+    """The main.cpp loop: host predictor (float32, TetMesh.h:319-348), solve from x = y
+    (VBD_GPU_Wrapper.cu:334) by the oracle, host velocity update (TetMesh.h:305-311)."""
+    dt32 = np.float32(dt)
+    dtsr = np.float32(1.0) / (dt32 * dt32)
+    x = m.x.astype(np.float32).copy()
+    v = m.v.astype(np.float32).copy()
+    free = m.fixed == 0
+    g = np.array([0.0, -9.8, 0.0], np.float32)
+    for _ in range(steps):
+        xprev = x.copy()
+        v[free] = v[free] + dt32 * g
+        y = x.copy()
+        y[free] = x[free] + dt32 * v[free]
+        x = po.solve(m, x, y, float(dtsr), iters, True, rho, init_from_inertia=True).astype(np.float32)
+        v[free] = ((x[free] - xprev[free]) / dt32) * np.float32(0.999)
+    return x
+
+
+def test_cpp_surface_matches_oracle(gpu_device, tmp_path):
+    m = meshgen.beam()
+    s = meshgen.BEAM_SETTINGS
+    out = run_cpp(m, s["iterations"], 10, s["dt"], s["rho"], tmp_path)
+    o = po.simulate(m, 10, s["dt"], s["iterations"], s["gravity"], True, s["rho"], precision=32)
+    assert rel_err(out["x1"], o["x"], m) < 1e-5
+    assert np.abs(out["v1"] - o["v"]).max() < 1e-3 * np.abs(o["v"]).max()
+    w = wrapper_flow_oracle(m, s["iterations"], 10, s["dt"], s["rho"])
+    assert rel_err(out["x2"], w, m) < 1e-5
+    assert out["ncol"] == 8
+    assert out["nsurf"] == 2 * 2 * (16 * 4 + 16 * 4 + 4 * 4)
+    lines = open(out["obj"]).read().splitlines()
+    assert sum(1 for ln in lines if ln.startswith("v ")) == m.num_verts
+    assert sum(1 for ln in lines if ln.startswith("f ")) == out["nsurf"]
+    # log-J elastic energy of the final state (VBDsolver::computeTotalEnergy)
+    mass, trv, dm, v0 = po.mesh_setup(m.rest, m.tets, m.density, precision=64)
+    X = out["x1"].astype(np.float64)
+    D = np.stack([X[m.tets[:, k]] - X[m.tets[:, 0]] for k in (1, 2, 3)], axis=2)
+    F = np.einsum("tij,tjk->tik", D, dm)
+    J = np.abs(np.linalg.det(F))
+    mu, lam = float(m.mu[0]), float(m.lam[0])
+    e = np.sum(v0 * (0.5 * mu * (np.einsum("tij,tij->t", F, F) - 3) - mu * np.log(J) + 0.5 * lam * np.log(J) ** 2))
+    assert abs(out["energy"] - e) <= 1e-4 * abs(e)
