@@ -154,6 +154,21 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def _lines(self):
+        try:
+            return open(self.path).read().splitlines()
+        except Exception:
+            return []
+
+    def wait_first_sample(self, timeout=5.0):
+        t0 = time.time()
+        while self.proc is not None and not self._lines() and time.time() - t0 < timeout:
+            time.sleep(0.05)
+
+    def mark(self):
+        """Samples from here on belong to the timed passes."""
+        self.first = len(self._lines())
+
     def stop(self):
         if self.proc is None:
             return None
@@ -163,7 +178,7 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         rows = []
-        for line in open(self.path):
+        for line in self._lines()[getattr(self, "first", 0):]:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -258,15 +273,19 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    # nvidia-smi needs about a second to start sampling: launch it before the warm-up so that its
+    # samples cover the timed passes
+    clocks = ClockSampler(local)
+    clocks.start()
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             solver.step(dt, iters, grav, True, rho)
         solver.sync()
+        clocks.wait_first_sample()
 
         # ---- timed region: device-resident steps, one event pair per step, L2 flushed between ----
-        clocks = ClockSampler(local)
         barrier()
-        clocks.start()
+        clocks.mark()
         launches0 = solver.kernel_launches()
         ms_total = 0.0
         for _ in range(args.steps):
@@ -323,12 +342,14 @@ def main():
 
     peak, peak_kind = measured_peaks()
     achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9 if sweep_ms > 0 else None
+    # DRAM traffic per launch: the ncu-measured traffic / algorithmic-bytes ratio of the sweep
+    # kernel (profiles/sweep_cube64_dram.txt) times this run's algorithmic bytes per launch
     traffic = None
     prof = os.path.join(ROOT, "profiles", "sweep_cube64_dram.txt")
-    if os.path.exists(prof):
+    if os.path.exists(prof) and sweep_launches:
         for line in open(prof):
-            if line.startswith("dram_bytes_per_launch"):
-                traffic = float(line.split("=")[1].split()[0])
+            if line.startswith("dram_traffic_over_algorithmic"):
+                traffic = float(line.split("=")[1].split()[0]) * sweep_bytes / sweep_launches
     alg_bytes_per_vi = None
     if sweep_launches:
         alg_bytes_per_vi = sweep_bytes / (mesh.num_verts * iters * args.steps)
