@@ -106,6 +106,17 @@ int vbd_solver_init(vbd_solver* s, int32_t num_verts, int32_t num_tets, const fl
                     const int32_t* group_offsets, const int32_t* group_vertices, const float* dm_inv,
                     const float* rest_vol, const float* tet_mu, const float* tet_lambda);
 
+/* Uploads a batch of independent meshes as one solver problem (no reference counterpart: the
+ * reference handles one mesh per VBD_GPU_Solver).  Arrays are the meshes' arrays concatenated;
+ * vert_offsets[M+1] / tet_offsets[M+1] delimit mesh m, and tets_local holds each mesh's own vertex
+ * ids (0-based within the mesh).  Each mesh is coloured with the greedy colouring of
+ * GraphColoring::colorVertices on its own; colour c of every mesh is swept by one launch.  Positions,
+ * velocities and inertia are then addressed in the concatenated numbering by every other call. */
+int vbd_solver_init_batch(vbd_solver* s, int32_t num_meshes, const int32_t* vert_offsets, const int32_t* tet_offsets,
+                          const float* positions, const float* velocities, const float* vertex_mass,
+                          const uint8_t* fixed, const int32_t* tets_local, const float* dm_inv, const float* rest_vol,
+                          const float* tet_mu, const float* tet_lambda);
+
 /* Per-tet materials (TetMesh::tetMu / tetLambda, TetMesh.h:31-32); either pointer may be
  * null to keep the current values. */
 int vbd_solver_set_materials(vbd_solver* s, const float* tet_mu, const float* tet_lambda);

@@ -31,3 +31,15 @@ def test_kuhn_split_is_conforming_and_fills_cells():
     _, counts = np.unique(faces, axis=0, return_counts=True)
     assert counts.max() == 2
     assert (counts == 1).sum() == 2 * (3 * 2 + 3 * 2 + 2 * 2) * 2
+
+
+def test_batched_config_sizes():
+    ms = meshgen.batched_blocks()
+    b = meshgen.concat(ms)
+    assert len(ms) == 512
+    assert 1.5e6 < b.num_verts < 1.9e6 and 7.5e6 < b.num_tets < 9.5e6
+    dims = np.array([m.dims for m in ms])
+    assert dims.min() >= 4 and dims.max() <= 24
+    assert all(m.fixed.sum() > 0 for m in ms)
+    E = np.array([m.meta["E"] for m in ms])
+    assert 1e4 <= E.min() and E.max() <= 1e6

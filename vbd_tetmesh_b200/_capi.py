@@ -54,6 +54,7 @@ SIGNATURES = {
     "vbd_solver_create": [C.POINTER(_p), C.c_int, _p],
     "vbd_solver_destroy": [_p],
     "vbd_solver_init": [_p, _i32, _i32, _p, _p, _p, _p, _p, _p, _i32, _p, _p, _p, _p, _p, _p],
+    "vbd_solver_init_batch": [_p, _i32, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p],
     "vbd_solver_set_materials": [_p, _p, _p],
     "vbd_solver_set_uniform_material": [_p, _f32, _f32],
     "vbd_solver_set_positions": [_p, _p],

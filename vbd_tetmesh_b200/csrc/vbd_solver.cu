@@ -645,6 +645,42 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     return VBD_OK;
 }
 
+int vbd_solver_init_batch(vbd_solver* s, int32_t M, const int32_t* voff, const int32_t* toff, const float* positions,
+                          const float* velocities, const float* vertex_mass, const uint8_t* fixed,
+                          const int32_t* tets_local, const float* dm_inv, const float* rest_vol, const float* tet_mu,
+                          const float* tet_lambda) {
+    vbd::clear_error();
+    if (!s) VBD_FAIL(VBD_ERR_INVALID_ARG, "null solver handle");
+    if (M <= 0 || !voff || !toff) VBD_FAIL(VBD_ERR_INVALID_ARG, "need num_meshes > 0 and the offset arrays");
+    if (voff[0] != 0 || toff[0] != 0) VBD_FAIL(VBD_ERR_INVALID_ARG, "offsets must start at 0");
+    for (int m = 0; m < M; ++m)
+        if (voff[m + 1] < voff[m] || toff[m + 1] < toff[m])
+            VBD_FAIL(VBD_ERR_INVALID_ARG, "offsets of mesh %d decrease", m);
+    const int32_t N = voff[M], T = toff[M];
+    if (T > 0 && !tets_local) VBD_FAIL(VBD_ERR_INVALID_ARG, "tets_local is null");
+    // global ids; each mesh's ids must stay inside its own vertex range
+    std::vector<int32_t> tets(4LL * T);
+    for (int m = 0; m < M; ++m) {
+        const int32_t nv = voff[m + 1] - voff[m];
+        for (int64_t k = 4LL * toff[m]; k < 4LL * toff[m + 1]; ++k) {
+            const int32_t id = tets_local[k];
+            if (id < 0 || id >= nv)
+                VBD_FAIL(VBD_ERR_INVALID_ARG, "mesh %d: tet %lld holds local vertex id %d outside [0, %d)", m,
+                         (long long)(k / 4), id, nv);
+            tets[k] = id + voff[m];
+        }
+    }
+    // Greedy colouring of the union: a vertex's neighbours all lie in its own mesh, so every mesh
+    // receives exactly its own GraphColoring::colorVertices assignment.
+    std::vector<int32_t> colour_of(N);
+    int32_t nc = 0;
+    VBD_TRY(vbd_color_vertices(N, T, tets.data(), colour_of.data(), &nc, 0, nullptr, nullptr));
+    std::vector<int32_t> offs(nc + 1), verts(N);
+    VBD_TRY(vbd_color_vertices(N, T, tets.data(), colour_of.data(), &nc, nc, offs.data(), verts.data()));
+    return vbd_solver_init(s, N, T, positions, velocities, nullptr, vertex_mass, fixed, tets.data(), nc, offs.data(),
+                           verts.data(), dm_inv, rest_vol, tet_mu, tet_lambda);
+}
+
 int vbd_solver_set_materials(vbd_solver* s, const float* tet_mu, const float* tet_lambda) {
     vbd::clear_error();
     VBD_TRY(need_ready(s));

@@ -132,3 +132,57 @@ def jittered_block(lx, ly, lz, cell=0.05, jitter=0.25, E=1e5, nu=0.3, density=10
 # Simulation settings of the configurations (dt, iterations, Chebyshev rho, steps, gravity).
 BEAM_SETTINGS = dict(dt=1.0 / 60.0, iterations=20, rho=0.95, steps=100, gravity=(0.0, -9.8, 0.0))
 CUBE_SETTINGS = dict(dt=1.0 / 120.0, iterations=50, rho=0.9, steps=20, gravity=(0.0, -9.8, 0.0))
+
+
+def batched_blocks(num_meshes=512, lo=4, hi=24, seed=2024, cell=0.05, jitter=0.25, density=1000.0):
+    """The batched configuration: num_meshes jittered grid blocks with dims drawn uniformly from the
+    integers [lo, hi]^3 (6 tets per cell), E log-uniform in [1e4, 1e6] Pa, nu uniform in [0.2, 0.45],
+    one random face pinned per mesh."""
+    rng = np.random.default_rng(seed)
+    faces = ("x0", "x1", "y0", "y1", "z0", "z1")
+    meshes = []
+    for k in range(num_meshes):
+        lx, ly, lz = (int(v) for v in rng.integers(lo, hi + 1, size=3))
+        E = float(10.0 ** rng.uniform(4.0, 6.0))
+        nu = float(rng.uniform(0.2, 0.45))
+        face = faces[int(rng.integers(0, 6))]
+        meshes.append(jittered_block(lx, ly, lz, cell=cell, jitter=jitter, E=E, nu=nu, density=density,
+                                     seed=seed * 1000 + k, pin_face=face))
+    return meshes
+
+
+@dataclass
+class Batch:
+    """Concatenation of meshes (mesh-local tet ids kept; vertex / tet offsets per mesh)."""
+
+    meshes: list
+    vert_offsets: np.ndarray
+    tet_offsets: np.ndarray
+    rest: np.ndarray
+    x: np.ndarray
+    v: np.ndarray
+    tets_local: np.ndarray
+    fixed: np.ndarray
+    mu: np.ndarray
+    lam: np.ndarray
+
+    @property
+    def num_verts(self):
+        return int(self.vert_offsets[-1])
+
+    @property
+    def num_tets(self):
+        return int(self.tet_offsets[-1])
+
+    def split(self, arr):
+        """Per-mesh slices of a (num_verts, ...) array."""
+        return [arr[self.vert_offsets[m]:self.vert_offsets[m + 1]] for m in range(len(self.meshes))]
+
+
+def concat(meshes) -> Batch:
+    vo = np.zeros(len(meshes) + 1, np.int32)
+    to = np.zeros(len(meshes) + 1, np.int32)
+    vo[1:] = np.cumsum([m.num_verts for m in meshes])
+    to[1:] = np.cumsum([m.num_tets for m in meshes])
+    cat = lambda name: np.concatenate([getattr(m, name) for m in meshes])  # noqa: E731
+    return Batch(meshes, vo, to, cat("rest"), cat("x"), cat("v"), cat("tets"), cat("fixed"), cat("mu"), cat("lam"))

@@ -243,3 +243,21 @@ def build_solver(mesh, device: int = 0, stream: int | None = None, lanes: int | 
     s.vertex_mass = mass
     s.colour_groups = (offs, verts)
     return s
+
+
+def build_batch_solver(batch, device: int = 0, stream: int | None = None) -> GPUSolver:
+    """One solver for a meshgen.Batch: per-mesh masses and rest-shape data on the host, then
+    vbd_solver_init_batch (per-mesh greedy colouring; colour c of all meshes in one launch)."""
+    mass = np.concatenate([mesh_mass(m.rest, m.tets, m.density)[0] for m in batch.meshes])
+    pre = [precompute_tets(m.rest, m.tets) for m in batch.meshes]
+    dminv = np.concatenate([p[0] for p in pre])
+    v0 = np.concatenate([p[1] for p in pre])
+    s = GPUSolver(device, stream)
+    keep = [np.ascontiguousarray(a) for a in (batch.vert_offsets, batch.tet_offsets)]
+    arrs = [_f32(batch.x, (-1, 3)), _f32(batch.v, (-1, 3)), _f32(mass), np.ascontiguousarray(batch.fixed, np.uint8),
+            _i32(batch.tets_local), _f32(dminv, (-1, 9)), _f32(v0), _f32(batch.mu), _f32(batch.lam)]
+    call("vbd_solver_init_batch", s._h, len(batch.meshes), _ptr(_i32(keep[0])), _ptr(_i32(keep[1])),
+         *[_ptr(a) for a in arrs])
+    s.num_verts, s.num_tets = batch.num_verts, batch.num_tets
+    s.vertex_mass = mass
+    return s
