@@ -160,6 +160,30 @@ int vbd_solver_solve_iteration(vbd_solver* s, float dt_sqr_reciprocal);
 int vbd_solver_step(vbd_solver* s, float dt, int32_t substeps, int32_t iterations, const float* gravity,
                     int32_t use_acceleration, float rho);
 
+/* ---- Adjoint (no reference counterpart) --------------------------------------------------------
+ * Gradients of a loss of the final state through a sequence of steps, each step implicitly
+ * differentiated as converged: (M/h^2 + H) lam = G is solved with the forward's coloured block
+ * Gauss-Seidel over per-vertex 3x3 blocks (off-diagonal blocks applied through per-tet products),
+ * then dL/dy = M/h^2 lam, dL/d(mu_t, lambda_t) -= lam . V (F - C) q_n and lam . V (J - 1) C q_n
+ * summed over the tet's vertices, and the adjoint flows through y = x + h v + h^2 g and
+ * v' = 0.999 (x' - x)/h to the previous step. */
+
+/* Starts recording the steps taken from now on (checkpoint_every > 0): the current positions and
+ * velocities, and those after every checkpoint_every-th sub-step, are kept on the device; steps in
+ * between are recomputed during the backward pass.  checkpoint_every = 0 stops recording.  The
+ * state must change only through vbd_solver_step while recording. */
+int vbd_solver_record(vbd_solver* s, int32_t checkpoint_every);
+
+/* Backward pass over every recorded sub-step: dl_dx / dl_dv (float[3N]; dl_dv may be null) are the
+ * loss gradient w.r.t. the final positions / velocities; writes dL/dx0, dL/dv0 (float[3N], at
+ * recording start) and dL/dmu, dL/dlambda (float[T], accumulated over all steps); any output may
+ * be null.  adjoint_iterations = Gauss-Seidel sweeps per step (warm-started from the previous
+ * step's lam), accelerated by the forward's Chebyshev weights for spectral-radius estimate
+ * adjoint_rho (0 = plain Gauss-Seidel).  The solver's own state is left as it was.  Completes
+ * before returning. */
+int vbd_solver_backward(vbd_solver* s, const float* dl_dx, const float* dl_dv, int32_t adjoint_iterations,
+                        float adjoint_rho, float* dl_dx0, float* dl_dv0, float* dl_dmu, float* dl_dlambda);
+
 /* Waits for all work queued on the handle's stream and reports sticky device errors, and
  * VBD_ERR_TIMEOUT if a grid barrier of the persistent kernel gave up since the last sync. */
 int vbd_solver_sync(vbd_solver* s);
@@ -204,7 +228,9 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *   VBD_OPT_BLOCK:       threads per block of the sweep kernel: 64, 128 or 256
  *   VBD_OPT_PERSISTENT:  1 = run each step / solve as one cooperative launch that walks the colours
  *                        with a grid barrier after each one (bounded wait: a barrier that gives up
- *                        makes the next vbd_solver_sync return VBD_ERR_TIMEOUT) */
+ *                        makes the next vbd_solver_sync return VBD_ERR_TIMEOUT)
+ *   VBD_OPT_ADJOINT_ALTERNATE: 1 = adjoint sweeps alternate the colour order (a forward and a
+ *                        backward sweep form one symmetric Gauss-Seidel pair) */
 typedef enum vbd_option {
     VBD_OPT_LANES = 0,
     VBD_OPT_LAYOUT = 1,
@@ -213,7 +239,8 @@ typedef enum vbd_option {
     VBD_OPT_PREFETCH = 4,
     VBD_OPT_PDL = 5,
     VBD_OPT_BLOCK = 6,
-    VBD_OPT_PERSISTENT = 7
+    VBD_OPT_PERSISTENT = 7,
+    VBD_OPT_ADJOINT_ALTERNATE = 8
 } vbd_option;
 int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value);
 int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value);

@@ -52,6 +52,9 @@ def lib():
         L.orc_handle_positions.restype = None
         L.orc_handle_destroy.argtypes = [_p]
         L.orc_handle_destroy.restype = None
+        L.orc_adjoint_f64.argtypes = [_i, _i, _p, _p, _p, _p, _p, _p, _p, _d, _d, _i, _p, _i, _d, _i, _p, _p, _p, _p,
+                                       _p, _p, _p, _p]
+        L.orc_adjoint_f64.restype = _i
         L.orc_num_threads_max.argtypes = []
         L.orc_num_threads_max.restype = _i
         _lib = L
@@ -156,6 +159,38 @@ def ip_energy(x, y, mass, tets, dminv, v0, mu, lam, h):
     return lib().orc_ip_energy(x.shape[0], tets.shape[0], _ptr(x), _ptr(y), _ptr(_d64(mass)), _ptr(tets),
                                _ptr(_d64(dminv, (-1, 9))), _ptr(_d64(v0)), _ptr(_d64(mu)), _ptr(_d64(lam)),
                                float(h))
+
+
+def adjoint_f64(mesh, steps, dt, iterations, dLdx_fn=None, gravity=(0.0, -9.8, 0.0), use_acceleration=True, rho=0.9,
+                x0=None, v0=None, mu=None, lam=None):
+    """FP64 forward (substeps 1) and implicit adjoint.  dLdx_fn(x_final) -> dL/dx_final (N,3).
+    Returns dict(x=final positions, gx0, gv0, gmu, glam, cg_iterations, residual)."""
+    rest = _d64(mesh.rest, (-1, 3))
+    x = _d64(mesh.x if x0 is None else x0, (-1, 3))
+    v = _d64(mesh.v if v0 is None else v0, (-1, 3))
+    tets = np.ascontiguousarray(mesh.tets, dtype=np.int32)
+    fixed = np.ascontiguousarray(mesh.fixed, dtype=np.uint8)
+    mu = _d64(mesh.mu if mu is None else mu)
+    lam = _d64(mesh.lam if lam is None else lam)
+    n, t = rest.shape[0], tets.shape[0]
+    g = _d64(gravity)
+    xf = np.empty((n, 3))
+    args = (n, t, _ptr(rest), _ptr(x), _ptr(v), _ptr(tets), _ptr(fixed), _ptr(mu), _ptr(lam), float(mesh.density),
+            float(dt), int(iterations), _ptr(g), int(bool(use_acceleration)), float(rho), int(steps))
+    if dLdx_fn is None:
+        lib().orc_adjoint_f64(*args, None, None, _ptr(xf), None, None, None, None, None)
+        return dict(x=xf)
+    # forward once to get the final state, then again with the loss gradient
+    lib().orc_adjoint_f64(*args, None, None, _ptr(xf), None, None, None, None, None)
+    dl = _d64(dLdx_fn(xf), (-1, 3))
+    gx0 = np.empty((n, 3))
+    gv0 = np.empty((n, 3))
+    gmu = np.empty(t)
+    glam = np.empty(t)
+    res = C.c_double(0.0)
+    it = lib().orc_adjoint_f64(*args, _ptr(dl), None, _ptr(xf), _ptr(gx0), _ptr(gv0), _ptr(gmu), _ptr(glam),
+                               C.byref(res))
+    return dict(x=xf, gx0=gx0, gv0=gv0, gmu=gmu, glam=glam, cg_iterations=it, residual=res.value)
 
 
 def max_threads():

@@ -575,6 +575,236 @@ template <class T> struct Sim {
     }
 };
 
+// ---- FP64 implicit adjoint of the step sequence (the reference gradient) -----------------------
+//
+// Each step is treated as converged: M/h^2 (x' - y) + dPsi/dx(x'; mu, lambda) = 0 on free vertices,
+// y = x + h v + h^2 g, v' = 0.999 (x' - x) / h, pinned vertices fixed.  Backward per step, with
+// X~, V~ the adjoints of (x', v'):
+//   G = X~ + c V~ (c = 0.999/h),  A_ff lam = G_f with A = M/h^2 + Hessian of Psi at x',
+//   y~ = M/h^2 lam,  x~ = y~ - c V~, v~ = h y~ (free),  x~_p = X~_p - (A_pf lam)_p, v~_p = V~_p,
+//   dL/dmu_e -= sum_n lam_n . V (F - C) q_n,  dL/dlambda_e -= sum_n lam_n . V (J - 1) C q_n.
+// A_ff lam = G is solved by conjugate gradients on the assembled block matrix (element Hessians
+// from the literal 12x12 form of Energy.cpp:115-154).
+struct AdjointF64 {
+    Sim<double> sim;
+    std::vector<std::vector<double>> xs, vs;  // positions / velocities at the start of each step, and the final state
+    // neighbour structure: for vertex i, sorted neighbour list including i, and block storage
+    std::vector<int32_t> nb_off, nb;
+    std::vector<double> blocks;  // 9 per (i, j) entry
+
+    int find(int i, int j) const {
+        const int32_t* b = nb.data() + nb_off[i];
+        const int n = nb_off[i + 1] - nb_off[i];
+        return nb_off[i] + int(std::lower_bound(b, b + n, j) - b);
+    }
+
+    void build_pattern() {
+        std::vector<std::vector<int32_t>> adj(sim.N);
+        for (int t = 0; t < sim.NT; ++t)
+            for (int a = 0; a < 4; ++a)
+                for (int b = 0; b < 4; ++b) adj[sim.tets[4 * t + a]].push_back(sim.tets[4 * t + b]);
+        nb_off.assign(sim.N + 1, 0);
+        nb.clear();
+        for (int i = 0; i < sim.N; ++i) {
+            adj[i].push_back(i);
+            std::sort(adj[i].begin(), adj[i].end());
+            adj[i].erase(std::unique(adj[i].begin(), adj[i].end()), adj[i].end());
+            nb.insert(nb.end(), adj[i].begin(), adj[i].end());
+            nb_off[i + 1] = (int)nb.size();
+        }
+    }
+
+    // full 12x12 element Hessian (as 16 3x3 blocks) and gradient, double
+    static void element(const M3<double>& Di, const M3<double>& F, double lam, double mu, double V, double H[4][4][3][3]) {
+        double J = det3(F);
+        M3<double> C = cofactor(F);
+        double Q[4][3];
+        q_rows(Di, Q);
+        double HF[9][9];
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                M3<double> dF{};
+                dF.m[i][j] = 1.0;
+                M3<double> dC = cofactor_deriv(F, dF);
+                for (int vj = 0; vj < 3; ++vj)
+                    for (int vi = 0; vi < 3; ++vi)
+                        HF[vi + 3 * vj][i + 3 * j] = mu * (dF.m[vi][vj] - dC.m[vi][vj]) + lam * C.m[i][j] * C.m[vi][vj] +
+                                                      lam * (J - 1.0) * dC.m[vi][vj];
+            }
+        for (int n = 0; n < 4; ++n)
+            for (int m = 0; m < 4; ++m)
+                for (int c = 0; c < 3; ++c)
+                    for (int cp = 0; cp < 3; ++cp) {
+                        double val = 0.0;
+                        for (int b = 0; b < 3; ++b)
+                            for (int d = 0; d < 3; ++d) val += HF[c + 3 * b][cp + 3 * d] * Q[n][b] * Q[m][d];
+                        H[n][m][c][cp] = V * val;
+                    }
+    }
+
+    M3<double> F_of(const std::vector<double>& x, int t) const {
+        M3<double> Ds = edge_matrix(x.data(), &sim.tets[4 * t]);
+        return matmul(Ds, sim.DmInv[t]);
+    }
+
+    void assemble(const std::vector<double>& x, double ih2) {
+        blocks.assign(nb.size() * 9, 0.0);
+        for (int i = 0; i < sim.N; ++i) {
+            const int k = find(i, i);
+            for (int c = 0; c < 3; ++c) blocks[9 * k + 4 * c] += sim.mass[i] * ih2;
+        }
+        double H[4][4][3][3];
+        for (int t = 0; t < sim.NT; ++t) {
+            element(sim.DmInv[t], F_of(x, t), sim.lam[t], sim.mu[t], sim.V0[t], H);
+            const int32_t* q = &sim.tets[4 * t];
+            for (int n = 0; n < 4; ++n)
+                for (int m = 0; m < 4; ++m) {
+                    const int k = find(q[n], q[m]);
+                    for (int c = 0; c < 3; ++c)
+                        for (int cp = 0; cp < 3; ++cp) blocks[9 * k + 3 * c + cp] += H[n][m][c][cp];
+                }
+        }
+    }
+
+    // y = A x restricted to rows/cols of the given mask (1 = included)
+    void matvec(const std::vector<double>& x, std::vector<double>& y, const std::vector<uint8_t>& row_mask,
+                const std::vector<uint8_t>& col_mask) const {
+        y.assign(3 * sim.N, 0.0);
+        for (int i = 0; i < sim.N; ++i) {
+            if (!row_mask[i]) continue;
+            for (int k = nb_off[i]; k < nb_off[i + 1]; ++k) {
+                const int j = nb[k];
+                if (!col_mask[j]) continue;
+                for (int c = 0; c < 3; ++c)
+                    for (int cp = 0; cp < 3; ++cp) y[3 * i + c] += blocks[9 * k + 3 * c + cp] * x[3 * j + cp];
+            }
+        }
+    }
+
+    int cg(const std::vector<double>& b, std::vector<double>& x, const std::vector<uint8_t>& mask, int maxit,
+           double tol) const {
+        x.assign(3 * sim.N, 0.0);
+        std::vector<double> r = b, p, Ap;
+        for (int i = 0; i < sim.N; ++i)
+            if (!mask[i]) r[3 * i] = r[3 * i + 1] = r[3 * i + 2] = 0.0;
+        p = r;
+        double rr = 0.0, bb = 0.0;
+        for (double v : r) rr += v * v;
+        bb = rr;
+        if (bb == 0.0) return 0;
+        int it = 0;
+        for (; it < maxit && rr > tol * tol * bb; ++it) {
+            matvec(p, Ap, mask, mask);
+            double pAp = 0.0;
+            for (size_t k = 0; k < p.size(); ++k) pAp += p[k] * Ap[k];
+            const double alpha = rr / pAp;
+            for (size_t k = 0; k < p.size(); ++k) {
+                x[k] += alpha * p[k];
+                r[k] -= alpha * Ap[k];
+            }
+            double rr2 = 0.0;
+            for (double v : r) rr2 += v * v;
+            const double beta = rr2 / rr;
+            rr = rr2;
+            for (size_t k = 0; k < p.size(); ++k) p[k] = r[k] + beta * p[k];
+        }
+        return it;
+    }
+
+    void forward(int steps, double dt, int iters, const double* g, bool accel, double rho) {
+        xs.clear();
+        vs.clear();
+        double gg[3] = {g[0], g[1], g[2]};
+        for (int k = 0; k < steps; ++k) {
+            xs.push_back(sim.x);
+            vs.push_back(sim.v);
+            sim.step(dt, 1, iters, gg, accel, rho, nullptr);
+        }
+        xs.push_back(sim.x);
+        vs.push_back(sim.v);
+    }
+
+    // Backward through all recorded steps.
+    int backward(double dt, const double* dLdx, const double* dLdv, double* gx0, double* gv0, double* gmu, double* glam,
+                 double* max_rel_residual) {
+        const int N = sim.N;
+        const double h = dt, ih2 = 1.0 / (h * h), c = 0.999 / h;
+        std::vector<double> ax(dLdx, dLdx + 3 * N), av(3 * N, 0.0);
+        if (dLdv) av.assign(dLdv, dLdv + 3 * N);
+        std::vector<double> gm(sim.NT, 0.0), gl(sim.NT, 0.0);
+        std::vector<uint8_t> freem(N), pinm(N);
+        for (int i = 0; i < N; ++i) {
+            freem[i] = sim.fixed[i] ? 0 : 1;
+            pinm[i] = sim.fixed[i] ? 1 : 0;
+        }
+        double worst = 0.0;
+        int total_it = 0;
+        const int steps = (int)xs.size() - 1;
+        for (int t = steps - 1; t >= 0; --t) {
+            const std::vector<double>& xn = xs[t + 1];
+            assemble(xn, ih2);
+            std::vector<double> G(3 * N, 0.0), lamv, Ap;
+            for (int i = 0; i < N; ++i)
+                for (int k = 0; k < 3; ++k) G[3 * i + k] = freem[i] ? ax[3 * i + k] + c * av[3 * i + k] : 0.0;
+            total_it += cg(G, lamv, freem, 20000, 1e-13);
+            // residual check
+            matvec(lamv, Ap, freem, freem);
+            double rn = 0.0, gn = 0.0;
+            for (int k = 0; k < 3 * N; ++k) {
+                rn += (Ap[k] - G[k]) * (Ap[k] - G[k]);
+                gn += G[k] * G[k];
+            }
+            if (gn > 0) worst = std::max(worst, std::sqrt(rn / gn));
+            // parameter gradients
+            for (int e = 0; e < sim.NT; ++e) {
+                const int32_t* q = &sim.tets[4 * e];
+                M3<double> F = F_of(xn, e);
+                M3<double> C = cofactor(F);
+                const double J = det3(F);
+                double Q[4][3];
+                q_rows(sim.DmInv[e], Q);
+                for (int n = 0; n < 4; ++n) {
+                    const int vi = q[n];
+                    if (!freem[vi]) continue;
+                    for (int r = 0; r < 3; ++r) {
+                        double fq = 0, cq = 0;
+                        for (int k = 0; k < 3; ++k) {
+                            fq += (F.m[r][k] - C.m[r][k]) * Q[n][k];
+                            cq += C.m[r][k] * Q[n][k];
+                        }
+                        gm[e] -= lamv[3 * vi + r] * sim.V0[e] * fq;
+                        gl[e] -= lamv[3 * vi + r] * sim.V0[e] * (J - 1.0) * cq;
+                    }
+                }
+            }
+            // pinned: x~_p = X~_p - (A_pf lam)_p
+            std::vector<double> Apf;
+            matvec(lamv, Apf, pinm, freem);
+            for (int i = 0; i < N; ++i)
+                for (int k = 0; k < 3; ++k) {
+                    const int d = 3 * i + k;
+                    if (freem[i]) {
+                        const double yb = sim.mass[i] * ih2 * lamv[d];
+                        ax[d] = yb - c * av[d];
+                        av[d] = h * yb;
+                    } else {
+                        ax[d] = ax[d] - Apf[d];
+                    }
+                }
+        }
+        for (int k = 0; k < 3 * N; ++k) {
+            gx0[k] = ax[k];
+            gv0[k] = av[k];
+        }
+        for (int e = 0; e < sim.NT; ++e) {
+            gmu[e] = gm[e];
+            glam[e] = gl[e];
+        }
+        if (max_rel_residual) *max_rel_residual = worst;
+        return total_it;
+    }
+};
+
 template <class T> static void to_T(const double* in, std::vector<T>& out, int n) {
     out.resize(n);
     for (int i = 0; i < n; ++i) out[i] = T(in[i]);
@@ -801,6 +1031,24 @@ void orc_handle_positions(void* h, double* x_out) {
 }
 
 void orc_handle_destroy(void* h) { delete static_cast<orc::Sim<float>*>(h); }
+
+// FP64 forward of `steps` steps (substeps 1) from (x0, v0) and the implicit adjoint of the final-state
+// loss gradient (dLdx, dLdv nullable): writes final positions, dL/dx0, dL/dv0, dL/dmu, dL/dlambda.
+int orc_adjoint_f64(int N, int NT, const double* rest, const double* x0, const double* v0, const int32_t* tets,
+                    const uint8_t* fixed, const double* tet_mu, const double* tet_lambda, double density, double dt,
+                    int iters, const double* g, int use_accel, double rho, int steps, const double* dLdx,
+                    const double* dLdv, double* x_final, double* gx0, double* gv0, double* gmu, double* glam,
+                    double* max_rel_residual) {
+    orc::AdjointF64 a;
+    a.sim.mode = orc::CLOSED;
+    a.sim.setup(N, NT, rest, x0, v0, tets, fixed, tet_mu, tet_lambda, density);
+    a.sim.color();
+    a.build_pattern();
+    a.forward(steps, dt, iters, g, use_accel != 0, rho);
+    for (int k = 0; k < 3 * N; ++k) x_final[k] = a.sim.x[k];
+    if (!dLdx) return 0;
+    return a.backward(dt, dLdx, dLdv, gx0, gv0, gmu, glam, max_rel_residual);
+}
 
 int orc_num_threads_max(void) {
 #ifdef _OPENMP

@@ -36,6 +36,7 @@ OPT_PREFETCH = 4
 OPT_PDL = 5
 OPT_BLOCK = 6
 OPT_PERSISTENT = 7
+OPT_ADJOINT_ALTERNATE = 8
 
 _p = C.c_void_p
 _i32 = C.c_int32
@@ -67,6 +68,8 @@ SIGNATURES = {
     "vbd_solver_solve_iteration": [_p, _f32],
     "vbd_solver_step": [_p, _f32, _i32, _i32, _p, _i32, _f32],
     "vbd_solver_sync": [_p],
+    "vbd_solver_record": [_p, _i32],
+    "vbd_solver_backward": [_p, _p, _p, _i32, _f32, _p, _p, _p, _p],
     "vbd_solver_energy": [_p, _i32, _f32, _PF64],
     "vbd_solver_status": [_p, _PI64, _PI32, _i32],
     "vbd_solver_set_option": [_p, _i32, _i32],

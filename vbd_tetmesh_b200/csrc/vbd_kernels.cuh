@@ -707,6 +707,364 @@ __global__ void k_pack_compact(const TetRec* __restrict__ rec, const int* __rest
     cmat[j] = make_float2(r.c.y * r.c.z, r.c.y * r.c.w);
 }
 
+// ---- implicit adjoint of a converged step --------------------------------------------------
+//
+// A step's positions x' solve M/h^2 (x' - y) + dPsi/dx(x') = 0 on free vertices.  Its adjoint
+// solves (M/h^2 + H(x')) lam = G by the same coloured block Gauss-Seidel as the forward: vertex i
+// sets lam_i = A_ii^-1 (G_i - sum_{j != i} A_ij lam_j), where the off-diagonal sum is applied per
+// tet as V dP(dF') q_i with dF' = sum_{k != i} lam_k q_k^T, dP = dP/dF[dF'] = mu (dF' - dC) +
+// lambda (C : dF') C + lambda (J - 1) dC, dC the directional derivative of cof F; A_ii is the
+// forward's exact diagonal block m/h^2 I + sum V (mu |q|^2 I + lambda (C q)(C q)^T).
+
+// The element seen from vertex v: the other three vertices, their rows q_k of Q = Ps Dm^-1, the
+// vertex's own row q_n, and (V mu, V lambda).
+struct ElemView {
+    int nb[3];
+    float q[3][3];
+    float qn[3];
+    float a, b;
+};
+
+__device__ __forceinline__ ElemView view_of(const TetRec& r, int v) {
+    const int ids[4] = {r.ids.x, r.ids.y, r.ids.z, r.ids.w};
+    const float D[3][3] = {{r.a.x, r.a.y, r.a.z}, {r.a.w, r.b.x, r.b.y}, {r.b.z, r.b.w, r.c.x}};
+    const int n = (ids[0] == v) ? 0 : (ids[1] == v) ? 1 : (ids[2] == v) ? 2 : 3;
+    ElemView e;
+    float Q[4][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        Q[0][c] = -D[0][c] - D[1][c] - D[2][c];
+        Q[1][c] = D[0][c];
+        Q[2][c] = D[1][c];
+        Q[3][c] = D[2][c];
+    }
+    int m = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (k == n) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) e.qn[c] = Q[k][c];
+        } else {
+            e.nb[m] = ids[k];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) e.q[m][c] = Q[k][c];
+            ++m;
+        }
+    }
+    e.a = r.c.y * r.c.z;
+    e.b = r.c.y * r.c.w;
+    return e;
+}
+
+__device__ __forceinline__ ElemView view_of(const CompactRec& r, int) {
+    ElemView e;
+    e.nb[0] = r.nb0;
+    e.nb[1] = r.nb1;
+    e.nb[2] = r.nb2;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) e.q[k][c] = r.q[3 * k + c];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) e.qn[c] = -(r.q[c] + r.q[3 + c] + r.q[6 + c]);
+    e.a = r.a;
+    e.b = r.b;
+    return e;
+}
+
+__device__ __forceinline__ void cof3(const float F[3][3], float C[3][3]) {
+    C[0][0] = F[1][1] * F[2][2] - F[1][2] * F[2][1];
+    C[0][1] = F[1][2] * F[2][0] - F[1][0] * F[2][2];
+    C[0][2] = F[1][0] * F[2][1] - F[1][1] * F[2][0];
+    C[1][0] = F[2][1] * F[0][2] - F[2][2] * F[0][1];
+    C[1][1] = F[2][2] * F[0][0] - F[2][0] * F[0][2];
+    C[1][2] = F[2][0] * F[0][1] - F[2][1] * F[0][0];
+    C[2][0] = F[0][1] * F[1][2] - F[0][2] * F[1][1];
+    C[2][1] = F[0][2] * F[1][0] - F[0][0] * F[1][2];
+    C[2][2] = F[0][0] * F[1][1] - F[0][1] * F[1][0];
+}
+
+// Directional derivative of the cofactor matrix: d/dt cof(F + t D) at t = 0.
+__device__ __forceinline__ void dcof3(const float F[3][3], const float D[3][3], float dC[3][3]) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+            dC[i][j] = D[i1][j1] * F[i2][j2] + F[i1][j1] * D[i2][j2] - D[i1][j2] * F[i2][j1] - F[i1][j2] * D[i2][j1];
+        }
+}
+
+// F, C, J of the element at positions X, seen from vertex v at xi.
+__device__ __forceinline__ void elem_F(const ElemView& e, float4 xi, const float4* __restrict__ X, float F[3][3],
+                                       float C[3][3], float& J) {
+    float d[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float4 p = X[e.nb[k]];
+        d[k][0] = p.x - xi.x;
+        d[k][1] = p.y - xi.y;
+        d[k][2] = p.z - xi.z;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) F[r][c] = d[0][r] * e.q[0][c] + d[1][r] * e.q[1][c] + d[2][r] * e.q[2][c];
+    cof3(F, C);
+    J = F[0][0] * C[0][0] + F[0][1] * C[0][1] + F[0][2] * C[0][2];
+}
+
+// Off-diagonal product of the element at vertex v: V dP(sum_{k != v} lam_k q_k^T) q_v.
+__device__ __forceinline__ void elem_offdiag(const ElemView& e, const float F[3][3], const float C[3][3], float J,
+                                             const float4* __restrict__ L, float out[3]) {
+    float dF[3][3];
+    float l[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float4 p = L[e.nb[k]];
+        l[k][0] = p.x;
+        l[k][1] = p.y;
+        l[k][2] = p.z;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dF[r][c] = l[0][r] * e.q[0][c] + l[1][r] * e.q[1][c] + l[2][r] * e.q[2][c];
+    float dC[3][3];
+    dcof3(F, dF, dC);
+    float dJ = 0.f;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dJ += C[r][c] * dF[r][c];
+    const float jm1 = J - 1.0f;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        float acc = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float dP = e.a * (dF[r][c] - dC[r][c]) + e.b * (dJ * C[r][c] + jm1 * dC[r][c]);
+            acc += dP * e.qn[c];
+        }
+        out[r] = acc;
+    }
+}
+
+struct AdjParams {
+    const float4* X;          // converged positions of the step
+    float4* lam;              // adjoint, updated in place (pinned entries stay 0)
+    const float4* G;          // right-hand side
+    const float4* y;          // w = mass
+    const int* inc_off;
+    const int* inc_tet;
+    const TetRec* rec;
+    const int4* crec;         // compact incidence records (when the forward uses them)
+    const float2* cmat;
+    float dtsr;
+    int v_begin, v_end;
+    float4* lam_next;         // Chebyshev: receives omega (lam~ - lam_pp) + lam_pp
+    float4* lam_pp;           // Chebyshev: adjoint before the previous sweep
+    float omega;
+    int accel;                // write lam_next
+    int keep_pp;              // store the pre-sweep adjoint into lam_pp
+};
+
+template <int LAYOUT> struct AdjElem;
+template <> struct AdjElem<0> {
+    using Rec = TetRec;
+    __device__ __forceinline__ static Rec fetch(const AdjParams& p, int j) { return load_rec(p.rec + __ldg(p.inc_tet + j)); }
+};
+template <> struct AdjElem<2> {
+    using Rec = CompactRec;
+    __device__ __forceinline__ static Rec fetch(const AdjParams& p, int j) { return load_compact(p.crec, p.cmat, j); }
+};
+
+// One colour of one adjoint Gauss-Seidel sweep.  LAYOUT 0 reads tet records through inc_tet,
+// LAYOUT 2 the forward's compact incidence records; the lane's first record is fetched before the
+// programmatic-launch dependency wait, the next one while the current is evaluated.
+template <int LANES, int LAYOUT>
+__global__ void __launch_bounds__(256) k_adj_sweep(AdjParams p) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & (LANES - 1);
+    const int v = p.v_begin + t / LANES;
+    const bool active = v < p.v_end;
+    int j0 = 0, j1 = 0;
+    if (active) {
+        j0 = __ldg(p.inc_off + v);
+        j1 = __ldg(p.inc_off + v + 1);
+    }
+    int j = j0 + lane;
+    typename AdjElem<LAYOUT>::Rec nxt;
+    if (j < j1) nxt = AdjElem<LAYOUT>::fetch(p, j);
+    pdl_trigger();
+    pdl_wait();
+    const float4 xi = active ? p.X[v] : make_float4(0.f, 0.f, 0.f, 0.f);
+    Acc acc;  // h.. = diagonal block, g. = off-diagonal product
+    acc.zero();
+    for (; j < j1; j += LANES) {
+        const typename AdjElem<LAYOUT>::Rec r = nxt;
+        if (j + LANES < j1) nxt = AdjElem<LAYOUT>::fetch(p, j + LANES);
+        const ElemView e = view_of(r, v);
+        float F[3][3], C[3][3], J;
+        elem_F(e, xi, p.X, F, C, J);
+        float o[3];
+        elem_offdiag(e, F, C, J, p.lam, o);
+        acc.g0 += o[0];
+        acc.g1 += o[1];
+        acc.g2 += o[2];
+        float Cq[3];
+#pragma unroll
+        for (int r2 = 0; r2 < 3; ++r2) Cq[r2] = C[r2][0] * e.qn[0] + C[r2][1] * e.qn[1] + C[r2][2] * e.qn[2];
+        const float am = e.a * (e.qn[0] * e.qn[0] + e.qn[1] * e.qn[1] + e.qn[2] * e.qn[2]);
+        acc.h00 += am + e.b * Cq[0] * Cq[0];
+        acc.h01 += e.b * Cq[0] * Cq[1];
+        acc.h02 += e.b * Cq[0] * Cq[2];
+        acc.h11 += am + e.b * Cq[1] * Cq[1];
+        acc.h12 += e.b * Cq[1] * Cq[2];
+        acc.h22 += am + e.b * Cq[2] * Cq[2];
+    }
+    group_reduce<LANES>(acc);
+    if (!active || lane != 0) return;
+    const float cm = p.y[v].w * p.dtsr;
+    const float4 g = p.G[v];
+    const float H00 = cm + acc.h00, H01 = acc.h01, H02 = acc.h02, H11 = cm + acc.h11, H12 = acc.h12, H22 = cm + acc.h22;
+    const float f0 = g.x - acc.g0, f1 = g.y - acc.g1, f2 = g.z - acc.g2;
+    const float A00 = H11 * H22 - H12 * H12, A01 = H02 * H12 - H01 * H22, A02 = H01 * H12 - H02 * H11;
+    const float A11 = H00 * H22 - H02 * H02, A12 = H02 * H01 - H00 * H12, A22 = H00 * H11 - H01 * H01;
+    const float det = H00 * A00 + H01 * A01 + H02 * A02;
+    float4 l = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (fabsf(det) > 1e-30f) {
+        const float inv = 1.0f / det;
+        l.x = inv * (A00 * f0 + A01 * f1 + A02 * f2);
+        l.y = inv * (A01 * f0 + A11 * f1 + A12 * f2);
+        l.z = inv * (A02 * f0 + A12 * f1 + A22 * f2);
+    }
+    const float4 lold = p.lam[v];
+    p.lam[v] = l;
+    if (p.accel) {
+        const float4 q = p.lam_pp[v];
+        p.lam_next[v] = make_float4(p.omega * (l.x - q.x) + q.x, p.omega * (l.y - q.y) + q.y,
+                                    p.omega * (l.z - q.z) + q.z, 0.f);
+    }
+    if (p.keep_pp) p.lam_pp[v] = lold;
+}
+
+// G = x~ + c v~ on free vertices [0, nfree).
+__global__ void k_adj_rhs(const float4* __restrict__ ax, const float4* __restrict__ av, float4* __restrict__ G, float c,
+                          int nfree) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfree) return;
+    const float4 a = ax[i], b = av[i];
+    G[i] = make_float4(a.x + c * b.x, a.y + c * b.y, a.z + c * b.z, 0.f);
+}
+
+// Pinned vertices [v_begin, v_end): x~_p -= sum_e V dP(sum_{k != p} lam_k q_k^T) q_p (their coupling
+// to the free vertices through the converged positions); v~_p unchanged.
+template <int LANES>
+__global__ void __launch_bounds__(256) k_adj_pinned(AdjParams p, float4* __restrict__ ax) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & (LANES - 1);
+    const int v = p.v_begin + t / LANES;
+    const bool active = v < p.v_end;
+    int j0 = 0, j1 = 0;
+    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (active) {
+        j0 = p.inc_off[v];
+        j1 = p.inc_off[v + 1];
+        xi = p.X[v];
+    }
+    Acc acc;
+    acc.zero();
+    for (int j = j0 + lane; j < j1; j += LANES) {
+        const TetRec r = load_rec(p.rec + p.inc_tet[j]);
+        const ElemView e = view_of(r, v);
+        float F[3][3], C[3][3], J;
+        elem_F(e, xi, p.X, F, C, J);
+        float o[3];
+        elem_offdiag(e, F, C, J, p.lam, o);
+        acc.g0 += o[0];
+        acc.g1 += o[1];
+        acc.g2 += o[2];
+    }
+    group_reduce<LANES>(acc);
+    if (!active || lane != 0) return;
+    float4 a = ax[v];
+    a.x -= acc.g0;
+    a.y -= acc.g1;
+    a.z -= acc.g2;
+    ax[v] = a;
+}
+
+// Free vertices: y~ = m/h^2 lam, x~ = y~ - c v~, v~ = h y~.
+__global__ void k_adj_update(const float4* __restrict__ lam, const float4* __restrict__ y, float4* __restrict__ ax,
+                             float4* __restrict__ av, float dtsr, float c, float h, int nfree) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfree) return;
+    const float4 l = lam[i];
+    const float cm = y[i].w * dtsr;
+    const float4 b = av[i];
+    const float yx = cm * l.x, yy = cm * l.y, yz = cm * l.z;
+    ax[i] = make_float4(yx - c * b.x, yy - c * b.y, yz - c * b.z, 0.f);
+    av[i] = make_float4(h * yx, h * yy, h * yz, 0.f);
+}
+
+// Per tet: dL/dmu -= sum_n lam_n . V (F - C) q_n, dL/dlambda -= sum_n lam_n . V (J - 1) C q_n
+// (accumulated over steps; lam of pinned vertices is 0).
+__global__ void k_adj_params(const TetRec* __restrict__ rec, const float4* __restrict__ X,
+                             const float4* __restrict__ lam, float* __restrict__ gmu, float* __restrict__ glam, int ntet) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntet) return;
+    const TetRec r = load_rec(rec + t);
+    const int ids[4] = {r.ids.x, r.ids.y, r.ids.z, r.ids.w};
+    const float D[3][3] = {{r.a.x, r.a.y, r.a.z}, {r.a.w, r.b.x, r.b.y}, {r.b.z, r.b.w, r.c.x}};
+    float Q[4][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        Q[0][c] = -D[0][c] - D[1][c] - D[2][c];
+        Q[1][c] = D[0][c];
+        Q[2][c] = D[1][c];
+        Q[3][c] = D[2][c];
+    }
+    float4 P[4], Lm[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        P[k] = X[ids[k]];
+        Lm[k] = lam[ids[k]];
+    }
+    float F[3][3];
+#pragma unroll
+    for (int rr = 0; rr < 3; ++rr) {
+        const float o = rr == 0 ? P[0].x : rr == 1 ? P[0].y : P[0].z;
+        const float e1 = (rr == 0 ? P[1].x : rr == 1 ? P[1].y : P[1].z) - o;
+        const float e2 = (rr == 0 ? P[2].x : rr == 1 ? P[2].y : P[2].z) - o;
+        const float e3 = (rr == 0 ? P[3].x : rr == 1 ? P[3].y : P[3].z) - o;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) F[rr][c] = e1 * D[0][c] + e2 * D[1][c] + e3 * D[2][c];
+    }
+    float C[3][3];
+    cof3(F, C);
+    const float J = F[0][0] * C[0][0] + F[0][1] * C[0][1] + F[0][2] * C[0][2];
+    float sm = 0.f, sl = 0.f;
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        const float l[3] = {Lm[n].x, Lm[n].y, Lm[n].z};
+#pragma unroll
+        for (int rr = 0; rr < 3; ++rr) {
+            float fq = 0.f, cq = 0.f;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                fq += (F[rr][c] - C[rr][c]) * Q[n][c];
+                cq += C[rr][c] * Q[n][c];
+            }
+            sm += l[rr] * fq;
+            sl += l[rr] * cq;
+        }
+    }
+    const float V = r.c.y;
+    gmu[t] -= V * sm;
+    glam[t] -= V * (J - 1.0f) * sl;
+}
+
 // ---- FP64 reductions (energies, residual) ---------------------------------------------------
 
 template <int BS>

@@ -122,6 +122,18 @@ struct vbd_solver {
     vbd::DBuf<float> d_omega;
     vbd::DBuf<vbd::GridBarrier> barrier;
     std::vector<float> omega_cache;
+    int adj_alternate = 0;  // adjoint sweeps alternate the colour order (symmetric Gauss-Seidel pairs)
+    // adjoint tape: sub-steps taken since vbd_solver_record, (x, v) every ckpt_every sub-steps
+    struct TapeStep {
+        float h, dtsr, hg[3], rho;
+        int iters, accel;
+    };
+    std::vector<TapeStep> tape;
+    int ckpt_every = 0;
+    std::vector<std::unique_ptr<vbd::DBuf<float4>>> ckpts;  // 2N each: x then v
+    vbd::DBuf<float4> adj_lam, adj_lam2, adj_lpp, adj_G, adj_ax, adj_av, adj_seg, adj_save;
+    vbd::DBuf<float> adj_gmu, adj_glam;
+    int adj_cur = 0;  // which of adj_lam / adj_lam2 holds lam
     long long launches = 0;
     std::vector<vbd::GraphEntry> graphs;
     std::vector<double> colour_bytes;               // algorithmic bytes of one sweep of colour c
@@ -335,6 +347,145 @@ struct vbd_solver {
         return check_launch();
     }
 
+    int snapshot(vbd::DBuf<float4>& dst) {
+        const size_t b4 = sizeof(float4) * (size_t)N;
+        CUDA_TRY(cudaMemcpyAsync(dst.p, x0.p, b4, cudaMemcpyDeviceToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(dst.p + N, v.p, b4, cudaMemcpyDeviceToDevice, stream));
+        return VBD_OK;
+    }
+
+    int record_substep(float h, float dtsr, const float* hg, int iters, bool accel, float rho) {
+        if (!ckpt_every) return VBD_OK;
+        TapeStep t{h, dtsr, {hg[0], hg[1], hg[2]}, rho, iters, accel ? 1 : 0};
+        tape.push_back(t);
+        if (tape.size() % (size_t)ckpt_every == 0) {
+            ckpts.emplace_back(new vbd::DBuf<float4>());
+            VBD_TRY(ckpts.back()->alloc(2 * (size_t)N));
+            VBD_TRY(snapshot(*ckpts.back()));
+        }
+        return VBD_OK;
+    }
+
+    // One recorded sub-step again, exactly as it ran (same launch sequence, hence same bits).
+    int replay_substep(const TapeStep& t) {
+        vbd::GraphKey key{};
+        key.kind = 0;
+        key.iters = t.iters;
+        key.accel = t.accel;
+        key.lanes = lanes;
+        key.layout = layout;
+        key.prefetch = prefetch;
+        key.pdl = pdl;
+        key.block = block;
+        key.h = t.h;
+        key.dtsr = t.dtsr;
+        key.hg[0] = t.hg[0];
+        key.hg[1] = t.hg[1];
+        key.hg[2] = t.hg[2];
+        key.rho = t.rho;
+        if (persistent && !timing)
+            return launch_persistent(t.iters, t.dtsr, t.accel != 0, t.rho, true, true, false, t.h, t.hg);
+        return run(key, [&] { return emit_substep(t.h, t.dtsr, t.hg, t.iters, t.accel != 0, t.rho); });
+    }
+
+    // Adjoint of one recorded sub-step whose converged positions are X: `sweeps` Gauss-Seidel
+    // sweeps on (M/h^2 + H) lam = x~ + c v~ with the Chebyshev blend of weight schedule
+    // getAcceleratorOmega(k, rho) (rho = 0: plain Gauss-Seidel), then the parameter gradients, the
+    // pinned-vertex coupling and the step's adjoint update.
+    int emit_adjoint_substep(const TapeStep& t, const float4* X, int sweeps, float rho) {
+        const float c = 0.999f / t.h;
+        const int L = lanes < 4 ? 4 : lanes;
+        vbd::k_adj_rhs<<<vbd::nblk(std::max(nfree, 1), 256), 256, 0, stream>>>(adj_ax.p, adj_av.p, adj_G.p, c, nfree);
+        VBD_TRY(check_launch());
+        int cur = adj_cur;
+        float omega = 1.0f;
+        const bool accel = rho > 0.0f;
+        for (int it = 1; it <= sweeps; ++it) {
+            bool blend = false;
+            if (accel) {
+                omega = vbd::omega_of(it, rho, omega);
+                blend = omega > 1.0f;
+            }
+            float4* lr = cur ? adj_lam2.p : adj_lam.p;
+            float4* lo = cur ? adj_lam.p : adj_lam2.p;
+            vbd::AdjParams ap{X,         lr,      adj_G.p, y.p,   inc_off.p,     inc_tet.p,     rec.p,
+                              crec.p,    cmat.p,  t.dtsr,  0,     0,             lo,            adj_lpp.p,
+                              omega,     blend ? 1 : 0,    accel ? 1 : 0};
+            const bool compact = layout == 2;
+            for (int k = 0; k < C; ++k) {
+                const int col = (adj_alternate && (it % 2 == 0)) ? C - 1 - k : k;
+                ap.v_begin = cstart[col];
+                ap.v_end = cstart[col + 1];
+                if (ap.v_end <= ap.v_begin) continue;
+                void (*fn)(vbd::AdjParams) = nullptr;
+                switch (L * 4 + (compact ? 2 : 0)) {
+                    case 16: fn = &vbd::k_adj_sweep<4, 0>; break;
+                    case 18: fn = &vbd::k_adj_sweep<4, 2>; break;
+                    case 32: fn = &vbd::k_adj_sweep<8, 0>; break;
+                    case 34: fn = &vbd::k_adj_sweep<8, 2>; break;
+                    case 64: fn = &vbd::k_adj_sweep<16, 0>; break;
+                    case 66: fn = &vbd::k_adj_sweep<16, 2>; break;
+                    case 128: fn = &vbd::k_adj_sweep<32, 0>; break;
+                    default: fn = &vbd::k_adj_sweep<32, 2>; break;
+                }
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3(vbd::nblk((long long)(ap.v_end - ap.v_begin) * L, 128));
+                cfg.blockDim = dim3(128);
+                cfg.stream = stream;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                attr[0].val.programmaticStreamSerializationAllowed = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = pdl ? 1 : 0;
+                CUDA_TRY(cudaLaunchKernelEx(&cfg, fn, ap));
+                VBD_TRY(check_launch());
+            }
+            if (blend) cur ^= 1;
+        }
+        float4* lam = cur ? adj_lam2.p : adj_lam.p;
+        if (T > 0) {
+            vbd::k_adj_params<<<vbd::nblk(T, 256), 256, 0, stream>>>(rec.p, X, lam, adj_gmu.p, adj_glam.p, T);
+            VBD_TRY(check_launch());
+        }
+        if (N > nfree) {
+            vbd::AdjParams ap{X,      lam,     adj_G.p, y.p,  inc_off.p, inc_tet.p, rec.p,
+                              crec.p, cmat.p,  t.dtsr,  nfree, N,        nullptr,   nullptr,
+                              1.0f,   0,       0};
+            const unsigned grid = vbd::nblk((long long)(N - nfree) * 8, 256);
+            vbd::k_adj_pinned<8><<<grid, 256, 0, stream>>>(ap, adj_ax.p);
+            VBD_TRY(check_launch());
+        }
+        if (nfree > 0) {
+            vbd::k_adj_update<<<vbd::nblk(nfree, 256), 256, 0, stream>>>(lam, y.p, adj_ax.p, adj_av.p, t.dtsr, c, t.h,
+                                                                      nfree);
+            VBD_TRY(check_launch());
+        }
+        return VBD_OK;
+    }
+
+    // The adjoint sequence of a sub-step is replayed as a graph keyed by its parameters, the
+    // positions slot it reads and which adjoint buffer is live.
+    int adjoint_substep(const TapeStep& t, int slot, const float4* X, int sweeps, float rho) {
+        vbd::GraphKey key{};
+        key.kind = 3 + slot;
+        key.iters = sweeps;
+        key.init = adj_cur;
+        key.lanes = lanes;
+        key.layout = layout;
+        key.pdl = pdl;
+        key.accel = adj_alternate;
+        key.h = t.h;
+        key.dtsr = t.dtsr;
+        key.rho = rho;
+        VBD_TRY(run(key, [&] { return emit_adjoint_substep(t, X, sweeps, rho); }));
+        float omega = 1.0f;
+        for (int it = 1; it <= sweeps && rho > 0.0f; ++it) {
+            omega = vbd::omega_of(it, rho, omega);
+            if (omega > 1.0f) adj_cur ^= 1;
+        }
+        return VBD_OK;
+    }
+
     template <class Emit> int run(const vbd::GraphKey& key, Emit emit) {
         if (!use_graph || timing) return emit();
         vbd::GraphEntry* hit = nullptr;
@@ -361,7 +512,7 @@ struct vbd_solver {
                 cudaGraphDestroy(g);
                 VBD_FAIL(VBD_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ie));
             }
-            if (graphs.size() >= 16) {
+            if (graphs.size() >= 64) {
                 cudaGraphExecDestroy(graphs.front().exec);
                 cudaGraphDestroy(graphs.front().graph);
                 graphs.erase(graphs.begin());
@@ -567,12 +718,14 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     // Incident tets of each free vertex, ascending tet id (TetMesh::vertAdjacentTets).
     std::vector<int32_t> voff(N + 1), vtets(4LL * T);
     vbd::build_vertex_tets(N, T, tets, voff.data(), vtets.data());
+    // Incident tets of every vertex (free ones first, so the sweeps' incidences are [0, ninc); the
+    // pinned vertices' lists serve the adjoint's coupling term).
     std::vector<int32_t> inc_off(N + 1, 0);
-    for (int i = 0; i < nfree; ++i) inc_off[i + 1] = inc_off[i] + (voff[perm[i] + 1] - voff[perm[i]]);
-    for (int i = nfree; i < N; ++i) inc_off[i + 1] = inc_off[i];
-    const long long ninc = inc_off[N];
-    std::vector<int32_t> inc_tet(std::max<long long>(ninc, 1)), inc_vertex(std::max<long long>(ninc, 1));
-    for (int i = 0; i < nfree; ++i) {
+    for (int i = 0; i < N; ++i) inc_off[i + 1] = inc_off[i] + (voff[perm[i] + 1] - voff[perm[i]]);
+    const long long ninc = inc_off[nfree];
+    const long long ninc_all = inc_off[N];
+    std::vector<int32_t> inc_tet(std::max<long long>(ninc_all, 1)), inc_vertex(std::max<long long>(ninc_all, 1));
+    for (int i = 0; i < N; ++i) {
         std::copy(vtets.begin() + voff[perm[i]], vtets.begin() + voff[perm[i] + 1], inc_tet.begin() + inc_off[i]);
         std::fill(inc_vertex.begin() + inc_off[i], inc_vertex.begin() + inc_off[i + 1], i);
     }
@@ -848,8 +1001,103 @@ int vbd_solver_step(vbd_solver* s, float dt, int32_t substeps, int32_t iteration
             VBD_TRY(s->launch_persistent(iterations, dtsr, use_acceleration != 0, rho, true, true, false, h, hg));
         else
             VBD_TRY(s->run(key, [&] { return s->emit_substep(h, dtsr, hg, iterations, use_acceleration != 0, rho); }));
+        VBD_TRY(s->record_substep(h, dtsr, hg, iterations, use_acceleration != 0, rho));
     }
     return VBD_OK;
+}
+
+int vbd_solver_record(vbd_solver* s, int32_t checkpoint_every) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (checkpoint_every < 0) VBD_FAIL(VBD_ERR_INVALID_ARG, "checkpoint_every must be >= 0");
+    DeviceScope scope(s->device);
+    s->tape.clear();
+    s->ckpts.clear();
+    s->ckpt_every = checkpoint_every;
+    if (checkpoint_every > 0) {
+        s->ckpts.emplace_back(new vbd::DBuf<float4>());
+        VBD_TRY(s->ckpts.back()->alloc(2 * (size_t)s->N));
+        VBD_TRY(s->snapshot(*s->ckpts.back()));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+    }
+    return VBD_OK;
+}
+
+int vbd_solver_backward(vbd_solver* s, const float* dl_dx, const float* dl_dv, int32_t adjoint_iterations,
+                        float adjoint_rho, float* dl_dx0, float* dl_dv0, float* dl_dmu, float* dl_dlambda) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (s->ckpt_every <= 0 || s->ckpts.empty()) VBD_FAIL(VBD_ERR_STATE, "nothing recorded: call vbd_solver_record first");
+    if (!dl_dx) VBD_FAIL(VBD_ERR_INVALID_ARG, "dl_dx is null");
+    if (adjoint_iterations < 1) VBD_FAIL(VBD_ERR_INVALID_ARG, "adjoint_iterations must be >= 1");
+    if (!(adjoint_rho >= 0.0f) || !(adjoint_rho < 1.0f)) VBD_FAIL(VBD_ERR_INVALID_ARG, "adjoint_rho must be in [0, 1)");
+    DeviceScope scope(s->device);
+    const int N = s->N, T = s->T, K = s->ckpt_every;
+    const size_t b4 = sizeof(float4) * (size_t)N;
+    // adjoint buffers; captured graphs bake their addresses, so any reallocation drops them
+    for (auto* b : {&s->adj_lam, &s->adj_lam2, &s->adj_lpp, &s->adj_G, &s->adj_ax, &s->adj_av})
+        if (b->n != (size_t)N) {
+            s->drop_graphs();
+            VBD_TRY(b->alloc(N));
+        }
+    if (s->adj_seg.n != (size_t)K * N) {
+        s->drop_graphs();
+        VBD_TRY(s->adj_seg.alloc((size_t)K * N));
+    }
+    if (s->adj_save.n != 6 * (size_t)N) VBD_TRY(s->adj_save.alloc(6 * (size_t)N));
+    if (s->adj_gmu.n != (size_t)std::max(T, 1)) {
+        s->drop_graphs();
+        VBD_TRY(s->adj_gmu.alloc(std::max(T, 1)));
+        VBD_TRY(s->adj_glam.alloc(std::max(T, 1)));
+    }
+    // keep the caller's state; the recompute overwrites it
+    float4* live[6] = {s->x0.p, s->x1.p, s->pp.p, s->y.p, s->v.p, s->xprev.p};
+    for (int k = 0; k < 6; ++k)
+        CUDA_TRY(cudaMemcpyAsync(s->adj_save.p + (size_t)k * N, live[k], b4, cudaMemcpyDeviceToDevice, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->adj_lam.p, 0, b4, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->adj_lam2.p, 0, b4, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->adj_lpp.p, 0, b4, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->adj_gmu.p, 0, sizeof(float) * s->adj_gmu.n, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->adj_glam.p, 0, sizeof(float) * s->adj_glam.n, s->stream));
+    s->adj_cur = 0;
+    VBD_TRY(s->upload3(dl_dx, s->adj_ax.p, nullptr));
+    if (dl_dv)
+        VBD_TRY(s->upload3(dl_dv, s->adj_av.p, nullptr));
+    else
+        CUDA_TRY(cudaMemsetAsync(s->adj_av.p, 0, b4, s->stream));
+    const int nsteps = (int)s->tape.size();
+    const int nseg = (nsteps + K - 1) / K;
+    int rc = VBD_OK;
+    for (int seg = nseg - 1; seg >= 0 && !rc; --seg) {
+        const int t0 = seg * K, t1 = std::min(nsteps, t0 + K);
+        vbd::DBuf<float4>& ck = *s->ckpts[seg];
+        CUDA_TRY(cudaMemcpyAsync(s->x0.p, ck.p, b4, cudaMemcpyDeviceToDevice, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(s->x1.p, ck.p, b4, cudaMemcpyDeviceToDevice, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(s->v.p, ck.p + N, b4, cudaMemcpyDeviceToDevice, s->stream));
+        for (int t = t0; t < t1 && !rc; ++t) {
+            rc = s->replay_substep(s->tape[t]);
+            if (!rc && cudaMemcpyAsync(s->adj_seg.p + (size_t)(t - t0) * N, s->x0.p, b4, cudaMemcpyDeviceToDevice,
+                                       s->stream) != cudaSuccess)
+                VBD_FAIL(VBD_ERR_CUDA, "segment copy failed");
+        }
+        for (int t = t1 - 1; t >= t0 && !rc; --t)
+            rc = s->adjoint_substep(s->tape[t], t - t0, s->adj_seg.p + (size_t)(t - t0) * N, adjoint_iterations,
+                                    adjoint_rho);
+    }
+    if (!rc) {
+        if (dl_dx0) rc = s->download3(s->adj_ax.p, dl_dx0);
+        if (!rc && dl_dv0) rc = s->download3(s->adj_av.p, dl_dv0);
+        if (!rc && dl_dmu && T > 0 &&
+            cudaMemcpyAsync(dl_dmu, s->adj_gmu.p, sizeof(float) * T, cudaMemcpyDefault, s->stream) != cudaSuccess)
+            rc = VBD_ERR_CUDA;
+        if (!rc && dl_dlambda && T > 0 &&
+            cudaMemcpyAsync(dl_dlambda, s->adj_glam.p, sizeof(float) * T, cudaMemcpyDefault, s->stream) != cudaSuccess)
+            rc = VBD_ERR_CUDA;
+    }
+    for (int k = 0; k < 6; ++k)
+        CUDA_TRY(cudaMemcpyAsync(live[k], s->adj_save.p + (size_t)k * N, b4, cudaMemcpyDeviceToDevice, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return rc;
 }
 
 int vbd_solver_sync(vbd_solver* s) {
@@ -961,6 +1209,9 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
         case VBD_OPT_PERSISTENT:
             s->persistent = value ? 1 : 0;
             return VBD_OK;
+        case VBD_OPT_ADJOINT_ALTERNATE:
+            s->adj_alternate = value ? 1 : 0;
+            return VBD_OK;
         case VBD_OPT_BLOCK:
             if (value != 64 && value != 128 && value != 256)
                 VBD_FAIL(VBD_ERR_INVALID_ARG, "block must be 64, 128 or 256");
@@ -997,6 +1248,7 @@ int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value) {
         case VBD_OPT_PDL: *value = s->pdl; return VBD_OK;
         case VBD_OPT_BLOCK: *value = s->block; return VBD_OK;
         case VBD_OPT_PERSISTENT: *value = s->persistent; return VBD_OK;
+        case VBD_OPT_ADJOINT_ALTERNATE: *value = s->adj_alternate; return VBD_OK;
         default: VBD_FAIL(VBD_ERR_INVALID_ARG, "unknown option %d", option);
     }
 }

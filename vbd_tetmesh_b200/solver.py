@@ -184,6 +184,24 @@ class GPUSolver:
     def sync(self) -> None:
         call("vbd_solver_sync", self._h)
 
+    # -- adjoint ----------------------------------------------------------------------------------
+    def record(self, checkpoint_every: int = 10) -> None:
+        """Start (k > 0) or stop (0) recording steps for the backward pass."""
+        call("vbd_solver_record", self._h, int(checkpoint_every))
+
+    def backward(self, dl_dx, dl_dv=None, adjoint_iterations: int = 50, adjoint_rho: float = 0.0):
+        """Gradients of a final-state loss through the recorded steps:
+        returns (dL/dx0 (N,3), dL/dv0 (N,3), dL/dmu (T,), dL/dlambda (T,))."""
+        dl_dx = _f32(dl_dx, (-1, 3))
+        dv = None if dl_dv is None else _f32(dl_dv, (-1, 3))
+        gx = np.empty((self.num_verts, 3), np.float32)
+        gv = np.empty((self.num_verts, 3), np.float32)
+        gm = np.empty(self.num_tets, np.float32)
+        gl = np.empty(self.num_tets, np.float32)
+        call("vbd_solver_backward", self._h, _ptr(dl_dx), _ptr(dv), int(adjoint_iterations), float(adjoint_rho),
+             _ptr(gx), _ptr(gv), _ptr(gm), _ptr(gl))
+        return gx, gv, gm, gl
+
     # -- diagnostics ------------------------------------------------------------------------------
     def energy(self, kind: int, h: float = 1.0) -> float:
         out = C.c_double(0.0)
