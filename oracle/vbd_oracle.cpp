@@ -1041,6 +1041,9 @@ int orc_adjoint_f64(int N, int NT, const double* rest, const double* x0, const d
                     double* max_rel_residual) {
     orc::AdjointF64 a;
     a.sim.mode = orc::CLOSED;
+#ifdef _OPENMP
+    a.sim.threads = omp_get_max_threads();
+#endif
     a.sim.setup(N, NT, rest, x0, v0, tets, fixed, tet_mu, tet_lambda, density);
     a.sim.color();
     a.build_pattern();

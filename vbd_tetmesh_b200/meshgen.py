@@ -186,3 +186,24 @@ def concat(meshes) -> Batch:
     to[1:] = np.cumsum([m.num_tets for m in meshes])
     cat = lambda name: np.concatenate([getattr(m, name) for m in meshes])  # noqa: E731
     return Batch(meshes, vo, to, cat("rest"), cat("x"), cat("v"), cat("tets"), cat("fixed"), cat("mu"), cat("lam"))
+
+
+def diff_beam(seed=33, sigma=0.2):
+    """The differentiated configuration: 32x8x8-cell beam (cell 0.05 m, x = 0 face pinned) with per-tet
+    log mu, log lambda ~ N(log of the E = 1e5, nu = 0.3 values, sigma); the loss vertices are the 5x5
+    subset (j, k in {0, 2, 4, 6, 8}) of the x = max face, with targets = rest position + N(0, 0.01 m).
+    Returns (mesh, tip vertex ids, targets (25, 3) float64)."""
+    m = beam(32, 8, 8, cell=0.05)
+    rng = np.random.default_rng(seed)
+    mu0, lam0 = lame(1e5, 0.3)
+    m.mu = np.exp(rng.normal(np.log(mu0), sigma, m.num_tets)).astype(np.float32)
+    m.lam = np.exp(rng.normal(np.log(lam0), sigma, m.num_tets)).astype(np.float32)
+    ijk = m.ijk
+    tip = np.flatnonzero((ijk[:, 0] == 32) & (ijk[:, 1] % 2 == 0) & (ijk[:, 2] % 2 == 0))
+    target = m.rest[tip].astype(np.float64) + rng.normal(0.0, 0.01, (len(tip), 3))
+    m.meta.update(kind="diff_beam", seed=seed, sigma=sigma)
+    return m, tip, target
+
+
+DIFF_SETTINGS = dict(dt=1.0 / 60.0, iterations=30, rho=0.95, steps=30, gravity=(0.0, -9.8, 0.0), checkpoint=10,
+                     adjoint_iterations=50, adjoint_rho=0.95)
