@@ -219,6 +219,11 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *                        1 = 64 B tet records copied into incidence order and streamed,
  *                        2 = compact 56 B incidence records streamed (other three vertex ids, their
  *                            rows of Ps Dm^-1, V0 mu, V0 lambda)
+ *                        3 = factored 52 B incidence records streamed (other three vertex ids,
+ *                            s = M q_n, w = cof(M) q_n, det M for M = their rows of Ps Dm^-1, and the
+ *                            material products): the element block without forming F or cof(F);
+ *                            the default
+ *                        Defaults: 8 lanes, layout 3, 64-thread blocks, prefetch, PDL, graphs.
  *   VBD_OPT_GRAPH:       1 = replay a captured CUDA graph per step, 0 = direct launches
  *   VBD_OPT_KERNEL_TIMING: 1 = launch directly and bracket every colour-sweep kernel with a CUDA
  *                        event pair on the handle's stream (read with vbd_solver_kernel_time)

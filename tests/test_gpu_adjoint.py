@@ -89,6 +89,24 @@ def test_adjoint_matches_finite_differences(gpu_device):
         assert err < GRAD_RTOL
 
 
+@pytest.mark.parametrize("layout", [0, 2, 3])
+def test_adjoint_record_layouts_agree(gpu_device, layout):
+    """The adjoint sweeps read the forward's record layout (gathered tet records, compact or
+    factored incidence records); every layout must give the FP64 oracle's gradients."""
+    m, W = setup_case(seed=5)
+    s = build_solver(m, layout=layout)
+    s.record(2)
+    steps, dt, iters = 3, 1 / 60, 300
+    for _ in range(steps):
+        s.step(dt, iters, (0.0, -9.8, 0.0), False, 0.0)
+    gx, gv, gm, gl = s.backward(W, None, 300)
+    s.close()
+    o = po.adjoint_f64(m, steps, dt, iters, lambda x: W, use_acceleration=False)
+    errs = dict(mu=rel(gm, o["gmu"]), lam=rel(gl, o["glam"]), x0=rel(gx, o["gx0"]), v0=rel(gv, o["gv0"]))
+    print(f"layout {layout} adjoint vs FP64 adjoint:", errs)
+    assert all(e < GRAD_RTOL for e in errs.values()), errs
+
+
 def test_checkpoint_interval_does_not_change_gradients(gpu_device):
     m, W = setup_case(seed=3)
     ref = gpu_grads(m, W, 6, 1 / 60, 20, True, 0.9, 1, 40)

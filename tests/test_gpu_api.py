@@ -247,7 +247,7 @@ def test_autotune_restores_state_and_keeps_parity(gpu_device):
     x0 = s.get_positions()
     v0 = s.get_velocities()
     chosen = s.autotune(1 / 120, iterations=5, repeats=1)
-    assert chosen["lanes"] in (2, 4, 8, 16) and chosen["layout"] in (0, 1, 2)
+    assert chosen["lanes"] in (2, 4, 8, 16) and chosen["layout"] in (0, 1, 2, 3)
     np.testing.assert_array_equal(s.get_positions(), x0)
     np.testing.assert_array_equal(s.get_velocities(), v0)
     assert s.status() == (0, False)

@@ -48,6 +48,7 @@ struct SweepParams {
     float omega;
     int accel;                 // write x^(k) = omega (x~ - pp) + pp to xnext (VBD.cpp:290-300)
     int keep_pp;               // store the pre-sweep position into pp (VBD.cpp:78,89)
+    const float* cam;          // V0 mu |q_n|^2 per incidence (layout 3; crec then holds factored records)
 };
 
 // Programmatic dependent launch: let the next kernel in the stream start its prologue now, and
@@ -269,6 +270,79 @@ __device__ __forceinline__ void compact_contrib(const CompactRec& r, float4 xi, 
     }
 }
 
+// Factored incidence record (layout 3), 48 B + 4 B per (vertex, tet) incidence.  With M the 3x3
+// matrix whose rows are q_k of the three other vertices (the compact record's q) and q_n their
+// negated sum, F = D M for D = [d_0 d_1 d_2], d_k = x_k - x_n.  Hence
+//   F q_n = D s,          s = M q_n
+//   C q_n = cof(D) w,     w = cof(M) q_n       (cof(D M) = cof(D) cof(M))
+//   J     = det(D) det(M)
+// and cof(D) has the columns d_1 x d_2, d_2 x d_0, d_0 x d_1.  The per-incidence constants s, w,
+// det M are packed once, so a sweep never forms F or cof(F): about 70 floating-point operations
+// per incidence instead of about 115.  Same element block as tet_contrib up to rounding.
+//   int4  {nb0 | n << 30, nb1, nb2, s0}
+//   float4{s1, s2, w0, w1}
+//   float4{w2, det M, V0 mu, V0 lambda}
+//   float  V0 mu |q_n|^2                        (separate stream)
+struct FactRec {
+    int nb0, nb1, nb2;
+    float s0, s1, s2, w0, w1, w2, detm, a, b, am;
+};
+
+__device__ __forceinline__ FactRec load_fact(const int4* __restrict__ crec, const float* __restrict__ cam, int j) {
+    const int4 w0 = __ldg(crec + 3 * j);
+    const float4 w1 = __ldg(reinterpret_cast<const float4*>(crec) + 3 * j + 1);
+    const float4 w2 = __ldg(reinterpret_cast<const float4*>(crec) + 3 * j + 2);
+    FactRec r;
+    r.nb0 = w0.x & kCompactIdMask;
+    r.nb1 = w0.y;
+    r.nb2 = w0.z;
+    r.s0 = __int_as_float(w0.w);
+    r.s1 = w1.x;
+    r.s2 = w1.y;
+    r.w0 = w1.z;
+    r.w1 = w1.w;
+    r.w2 = w2.x;
+    r.detm = w2.y;
+    r.a = w2.z;
+    r.b = w2.w;
+    r.am = __ldg(cam + j);
+    return r;
+}
+
+template <bool WANT_H, bool COHERENT = false>
+__device__ __forceinline__ void fact_contrib(const FactRec& r, float4 xi, const float4* __restrict__ X, Acc& acc) {
+    const float4 p0 = load_pos<COHERENT>(X, r.nb0);
+    const float4 p1 = load_pos<COHERENT>(X, r.nb1);
+    const float4 p2 = load_pos<COHERENT>(X, r.nb2);
+    const float d0x = p0.x - xi.x, d0y = p0.y - xi.y, d0z = p0.z - xi.z;
+    const float d1x = p1.x - xi.x, d1y = p1.y - xi.y, d1z = p1.z - xi.z;
+    const float d2x = p2.x - xi.x, d2y = p2.y - xi.y, d2z = p2.z - xi.z;
+    // columns of cof(D)
+    const float c0x = d1y * d2z - d1z * d2y, c0y = d1z * d2x - d1x * d2z, c0z = d1x * d2y - d1y * d2x;
+    const float c1x = d2y * d0z - d2z * d0y, c1y = d2z * d0x - d2x * d0z, c1z = d2x * d0y - d2y * d0x;
+    const float c2x = d0y * d1z - d0z * d1y, c2y = d0z * d1x - d0x * d1z, c2z = d0x * d1y - d0y * d1x;
+    const float J = (d0x * c0x + d0y * c0y + d0z * c0z) * r.detm;
+    const float Fq0 = d0x * r.s0 + d1x * r.s1 + d2x * r.s2;
+    const float Fq1 = d0y * r.s0 + d1y * r.s1 + d2y * r.s2;
+    const float Fq2 = d0z * r.s0 + d1z * r.s1 + d2z * r.s2;
+    const float Cq0 = c0x * r.w0 + c1x * r.w1 + c2x * r.w2;
+    const float Cq1 = c0y * r.w0 + c1y * r.w1 + c2y * r.w2;
+    const float Cq2 = c0z * r.w0 + c1z * r.w1 + c2z * r.w2;
+    const float bj = r.b * (J - 1.0f);
+    acc.g0 += r.a * (Fq0 - Cq0) + bj * Cq0;
+    acc.g1 += r.a * (Fq1 - Cq1) + bj * Cq1;
+    acc.g2 += r.a * (Fq2 - Cq2) + bj * Cq2;
+    if (WANT_H) {
+        const float b0 = r.b * Cq0, b1 = r.b * Cq1, b2 = r.b * Cq2;
+        acc.h00 += r.am + b0 * Cq0;
+        acc.h01 += b0 * Cq1;
+        acc.h02 += b0 * Cq2;
+        acc.h11 += r.am + b1 * Cq1;
+        acc.h12 += b1 * Cq2;
+        acc.h22 += r.am + b2 * Cq2;
+    }
+}
+
 template <int LANES>
 __device__ __forceinline__ void group_reduce(Acc& a) {
 #pragma unroll
@@ -287,7 +361,7 @@ __device__ __forceinline__ void group_reduce(Acc& a) {
 
 // Element data of incidence j under each record layout:
 //   0 = tet record gathered through inc_tet, 1 = tet record streamed in incidence order,
-//   2 = compact streamed record.
+//   2 = compact streamed record, 3 = factored streamed record.
 template <int LAYOUT> struct Elem;
 template <> struct Elem<0> {
     using Rec = TetRec;
@@ -313,6 +387,14 @@ template <> struct Elem<2> {
     template <bool COHERENT>
     __device__ __forceinline__ static void contrib(const Rec& r, int, float4 xi, const float4* X, Acc& acc) {
         compact_contrib<true, COHERENT>(r, xi, X, acc);
+    }
+};
+template <> struct Elem<3> {
+    using Rec = FactRec;
+    __device__ __forceinline__ static Rec fetch(const SweepParams& p, int j) { return load_fact(p.crec, p.cam, j); }
+    template <bool COHERENT>
+    __device__ __forceinline__ static void contrib(const Rec& r, int, float4 xi, const float4* X, Acc& acc) {
+        fact_contrib<true, COHERENT>(r, xi, X, acc);
     }
 };
 
@@ -707,6 +789,61 @@ __global__ void k_pack_compact(const TetRec* __restrict__ rec, const int* __rest
     cmat[j] = make_float2(r.c.y * r.c.z, r.c.y * r.c.w);
 }
 
+// Factored records (layout 3) from the tet records: M's rows in the compact record's order, then
+// s = M q_n, w = cof(M) q_n, det M and the material products.
+__global__ void k_pack_factored(const TetRec* __restrict__ rec, const int* __restrict__ inc_tet,
+                                const int* __restrict__ inc_vertex, int4* __restrict__ crec, float* __restrict__ cam,
+                                int ninc) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ninc) return;
+    const TetRec r = rec[inc_tet[j]];
+    const int v = inc_vertex[j];
+    const int ids[4] = {r.ids.x, r.ids.y, r.ids.z, r.ids.w};
+    const float D[3][3] = {{r.a.x, r.a.y, r.a.z}, {r.a.w, r.b.x, r.b.y}, {r.b.z, r.b.w, r.c.x}};
+    float Q[4][3];
+    for (int c = 0; c < 3; ++c) {
+        Q[0][c] = -D[0][c] - D[1][c] - D[2][c];
+        for (int k = 1; k < 4; ++k) Q[k][c] = D[k - 1][c];
+    }
+    int n = 3;
+    for (int k = 0; k < 4; ++k)
+        if (ids[k] == v) {
+            n = k;
+            break;
+        }
+    int nb[3];
+    float M[3][3];
+    int m = 0;
+    for (int k = 0; k < 4; ++k) {
+        if (k == n) continue;
+        nb[m] = ids[k];
+        for (int c = 0; c < 3; ++c) M[m][c] = Q[k][c];
+        ++m;
+    }
+    const float q[3] = {-(M[0][0] + M[1][0] + M[2][0]), -(M[0][1] + M[1][1] + M[2][1]), -(M[0][2] + M[1][2] + M[2][2])};
+    float cof[3][3];
+    cof[0][0] = M[1][1] * M[2][2] - M[1][2] * M[2][1];
+    cof[0][1] = M[1][2] * M[2][0] - M[1][0] * M[2][2];
+    cof[0][2] = M[1][0] * M[2][1] - M[1][1] * M[2][0];
+    cof[1][0] = M[2][1] * M[0][2] - M[2][2] * M[0][1];
+    cof[1][1] = M[2][2] * M[0][0] - M[2][0] * M[0][2];
+    cof[1][2] = M[2][0] * M[0][1] - M[2][1] * M[0][0];
+    cof[2][0] = M[0][1] * M[1][2] - M[0][2] * M[1][1];
+    cof[2][1] = M[0][2] * M[1][0] - M[0][0] * M[1][2];
+    cof[2][2] = M[0][0] * M[1][1] - M[0][1] * M[1][0];
+    float sv[3], wv[3];
+    for (int i = 0; i < 3; ++i) {
+        sv[i] = M[i][0] * q[0] + M[i][1] * q[1] + M[i][2] * q[2];
+        wv[i] = cof[i][0] * q[0] + cof[i][1] * q[1] + cof[i][2] * q[2];
+    }
+    const float detm = M[0][0] * cof[0][0] + M[0][1] * cof[0][1] + M[0][2] * cof[0][2];
+    const float a = r.c.y * r.c.z, b = r.c.y * r.c.w;
+    crec[3 * j] = make_int4(nb[0] | (n << 30), nb[1], nb[2], __float_as_int(sv[0]));
+    crec[3 * j + 1] = make_int4(__float_as_int(sv[1]), __float_as_int(sv[2]), __float_as_int(wv[0]), __float_as_int(wv[1]));
+    crec[3 * j + 2] = make_int4(__float_as_int(wv[2]), __float_as_int(detm), __float_as_int(a), __float_as_int(b));
+    cam[j] = a * (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+}
+
 // ---- implicit adjoint of a converged step --------------------------------------------------
 //
 // A step's positions x' solve M/h^2 (x' - y) + dPsi/dx(x') = 0 on free vertices.  Its adjoint
@@ -867,6 +1004,7 @@ struct AdjParams {
     float omega;
     int accel;                // write lam_next
     int keep_pp;              // store the pre-sweep adjoint into lam_pp
+    const float* cam;         // factored records' V0 mu |q_n|^2 (layout 3; crec holds factored records)
 };
 
 template <int LAYOUT> struct AdjElem;
@@ -878,6 +1016,58 @@ template <> struct AdjElem<2> {
     using Rec = CompactRec;
     __device__ __forceinline__ static Rec fetch(const AdjParams& p, int j) { return load_compact(p.crec, p.cmat, j); }
 };
+template <> struct AdjElem<3> {
+    using Rec = FactRec;
+    __device__ __forceinline__ static Rec fetch(const AdjParams& p, int j) { return load_fact(p.crec, p.cam, j); }
+};
+
+// Adjoint element terms from a factored record (F = D M, dF = L M with L = [lam_0 lam_1 lam_2]):
+//   dF q_n = L s,   dC q_n = dcof(D)[L] w,   dJ = C : dF = det M sum_k c_k . lam_k
+// with c_k the columns of cof(D) and dcof(D)[L] the columns lam_1 x d_2 + d_1 x lam_2 (and
+// cyclic); off-diagonal product V dP(dF) q_n = a (dF q_n - dC q_n) + b (dJ C q_n + (J - 1) dC q_n),
+// diagonal block am I + b (C q_n)(C q_n)^T.
+__device__ __forceinline__ void fact_adjoint(const FactRec& r, float4 xi, const float4* __restrict__ X,
+                                             const float4* __restrict__ L, Acc& acc) {
+    const float4 p0 = X[r.nb0], p1 = X[r.nb1], p2 = X[r.nb2];
+    const float4 l0 = L[r.nb0], l1 = L[r.nb1], l2 = L[r.nb2];
+    const float d0[3] = {p0.x - xi.x, p0.y - xi.y, p0.z - xi.z};
+    const float d1[3] = {p1.x - xi.x, p1.y - xi.y, p1.z - xi.z};
+    const float d2[3] = {p2.x - xi.x, p2.y - xi.y, p2.z - xi.z};
+    const float m0[3] = {l0.x, l0.y, l0.z}, m1[3] = {l1.x, l1.y, l1.z}, m2[3] = {l2.x, l2.y, l2.z};
+    float c0[3], c1[3], c2[3], e0[3], e1[3], e2[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+        c0[i] = d1[i1] * d2[i2] - d1[i2] * d2[i1];
+        c1[i] = d2[i1] * d0[i2] - d2[i2] * d0[i1];
+        c2[i] = d0[i1] * d1[i2] - d0[i2] * d1[i1];
+        e0[i] = (m1[i1] * d2[i2] - m1[i2] * d2[i1]) + (d1[i1] * m2[i2] - d1[i2] * m2[i1]);
+        e1[i] = (m2[i1] * d0[i2] - m2[i2] * d0[i1]) + (d2[i1] * m0[i2] - d2[i2] * m0[i1]);
+        e2[i] = (m0[i1] * d1[i2] - m0[i2] * d1[i1]) + (d0[i1] * m1[i2] - d0[i2] * m1[i1]);
+    }
+    const float J = (d0[0] * c0[0] + d0[1] * c0[1] + d0[2] * c0[2]) * r.detm;
+    const float dJ = r.detm * ((c0[0] * m0[0] + c0[1] * m0[1] + c0[2] * m0[2]) +
+                               (c1[0] * m1[0] + c1[1] * m1[1] + c1[2] * m1[2]) +
+                               (c2[0] * m2[0] + c2[1] * m2[1] + c2[2] * m2[2]));
+    const float jm1 = J - 1.0f;
+    float o[3], Cq[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        Cq[i] = c0[i] * r.w0 + c1[i] * r.w1 + c2[i] * r.w2;
+        const float dFq = m0[i] * r.s0 + m1[i] * r.s1 + m2[i] * r.s2;
+        const float dCq = e0[i] * r.w0 + e1[i] * r.w1 + e2[i] * r.w2;
+        o[i] = r.a * (dFq - dCq) + r.b * (dJ * Cq[i] + jm1 * dCq);
+    }
+    acc.g0 += o[0];
+    acc.g1 += o[1];
+    acc.g2 += o[2];
+    acc.h00 += r.am + r.b * Cq[0] * Cq[0];
+    acc.h01 += r.b * Cq[0] * Cq[1];
+    acc.h02 += r.b * Cq[0] * Cq[2];
+    acc.h11 += r.am + r.b * Cq[1] * Cq[1];
+    acc.h12 += r.b * Cq[1] * Cq[2];
+    acc.h22 += r.am + r.b * Cq[2] * Cq[2];
+}
 
 // One colour of one adjoint Gauss-Seidel sweep.  LAYOUT 0 reads tet records through inc_tet,
 // LAYOUT 2 the forward's compact incidence records; the lane's first record is fetched before the
@@ -904,6 +1094,10 @@ __global__ void __launch_bounds__(256) k_adj_sweep(AdjParams p) {
     for (; j < j1; j += LANES) {
         const typename AdjElem<LAYOUT>::Rec r = nxt;
         if (j + LANES < j1) nxt = AdjElem<LAYOUT>::fetch(p, j + LANES);
+        if constexpr (LAYOUT == 3) {
+            fact_adjoint(r, xi, p.X, p.lam, acc);
+            continue;
+        } else {
         const ElemView e = view_of(r, v);
         float F[3][3], C[3][3], J;
         elem_F(e, xi, p.X, F, C, J);
@@ -922,6 +1116,7 @@ __global__ void __launch_bounds__(256) k_adj_sweep(AdjParams p) {
         acc.h11 += am + e.b * Cq[1] * Cq[1];
         acc.h12 += e.b * Cq[1] * Cq[2];
         acc.h22 += am + e.b * Cq[2] * Cq[2];
+        }
     }
     group_reduce<LANES>(acc);
     if (!active || lane != 0) return;

@@ -64,7 +64,8 @@ template <int L> static SweepFn pick_sweep(int layout, bool prefetch) {
     switch (layout) {
         case 0: return prefetch ? &k_sweep<L, 0, true> : &k_sweep<L, 0, false>;
         case 1: return prefetch ? &k_sweep<L, 1, true> : &k_sweep<L, 1, false>;
-        default: return prefetch ? &k_sweep<L, 2, true> : &k_sweep<L, 2, false>;
+        case 2: return prefetch ? &k_sweep<L, 2, true> : &k_sweep<L, 2, false>;
+        default: return prefetch ? &k_sweep<L, 3, true> : &k_sweep<L, 3, false>;
     }
 }
 
@@ -107,15 +108,16 @@ struct vbd_solver {
     vbd::DBuf<float4> x0, x1, pp, y, v, xprev;
     vbd::DBuf<int> perm, inc_off, inc_tet;
     vbd::DBuf<vbd::TetRec> rec, irec;
-    vbd::DBuf<int4> crec;                           // compact incidence records (layout 2)
+    vbd::DBuf<int4> crec;                           // compact (layout 2) or factored (layout 3) records
     vbd::DBuf<float2> cmat;
+    vbd::DBuf<float> cam;                           // factored layout: V0 mu |q_n|^2 per incidence
     vbd::DBuf<int> inc_vertex;                      // internal vertex of each incidence
     vbd::DBuf<float> stage, mat_stage;
     vbd::DBuf<unsigned long long> status;
     vbd::DBuf<double> partials, scalar;
     // defaults: the fastest shape measured on the 64^3 cube (compact streamed records, 4 lanes per
     // vertex, record prefetch, programmatic dependent launch, 128-thread blocks)
-    int lanes = 4, layout = 2, use_graph = 1, timing = 0, prefetch = 1, pdl = 1, block = 128;
+    int lanes = 8, layout = 3, use_graph = 1, timing = 0, prefetch = 1, pdl = 1, block = 64;
     int persistent = 0;                             // whole step in one cooperative launch
     long long spin_limit = 1LL << 22;               // barrier polls before a persistent launch gives up
     vbd::DBuf<int> d_cstart;
@@ -199,7 +201,7 @@ struct vbd_solver {
         if (ve <= vb) return VBD_OK;
         vbd::SweepParams p{xr,     xn,     pp.p,     y.p, inc_off.p, inc_tet.p, rec.p,          irec.p,
                            crec.p, cmat.p, status.p, vb,  ve,        dtsr,      omega, accel ? 1 : 0,
-                           keep_pp ? 1 : 0};
+                           keep_pp ? 1 : 0, cam.p};
         const long long threads = (long long)(ve - vb) * lanes;
         vbd::SweepFn fn = vbd::pick_sweep(lanes, layout, prefetch != 0);
         cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -303,15 +305,19 @@ struct vbd_solver {
             case 16: fn = &vbd::k_persistent<4, 0>; break;
             case 17: fn = &vbd::k_persistent<4, 1>; break;
             case 18: fn = &vbd::k_persistent<4, 2>; break;
+            case 19: fn = &vbd::k_persistent<4, 3>; break;
             case 32: fn = &vbd::k_persistent<8, 0>; break;
             case 33: fn = &vbd::k_persistent<8, 1>; break;
             case 34: fn = &vbd::k_persistent<8, 2>; break;
+            case 35: fn = &vbd::k_persistent<8, 3>; break;
             case 64: fn = &vbd::k_persistent<16, 0>; break;
             case 65: fn = &vbd::k_persistent<16, 1>; break;
             case 66: fn = &vbd::k_persistent<16, 2>; break;
+            case 67: fn = &vbd::k_persistent<16, 3>; break;
             case 128: fn = &vbd::k_persistent<32, 0>; break;
             case 129: fn = &vbd::k_persistent<32, 1>; break;
-            default: fn = &vbd::k_persistent<32, 2>; break;
+            case 130: fn = &vbd::k_persistent<32, 2>; break;
+            default: fn = &vbd::k_persistent<32, 3>; break;
         }
         int per_sm = 0, sms = 0;
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0));
@@ -320,7 +326,7 @@ struct vbd_solver {
         const int grid = per_sm * sms;
         vbd::PersistParams pp_{};
         pp_.sw = vbd::SweepParams{x0.p, x1.p, pp.p, y.p,  inc_off.p, inc_tet.p, rec.p, irec.p, crec.p, cmat.p,
-                                  status.p, 0,  0,    dtsr, 1.0f,      0,         accel ? 1 : 0};
+                                  status.p, 0,  0,    dtsr, 1.0f,      0,         accel ? 1 : 0, cam.p};
         pp_.xa = x0.p;
         pp_.xb = x1.p;
         pp_.v = v.p;
@@ -410,23 +416,27 @@ struct vbd_solver {
             float4* lo = cur ? adj_lam.p : adj_lam2.p;
             vbd::AdjParams ap{X,         lr,      adj_G.p, y.p,   inc_off.p,     inc_tet.p,     rec.p,
                               crec.p,    cmat.p,  t.dtsr,  0,     0,             lo,            adj_lpp.p,
-                              omega,     blend ? 1 : 0,    accel ? 1 : 0};
-            const bool compact = layout == 2;
+                              omega,     blend ? 1 : 0,    accel ? 1 : 0, cam.p};
+            const int alay = (layout == 2 || layout == 3) ? layout : 0;
             for (int k = 0; k < C; ++k) {
                 const int col = (adj_alternate && (it % 2 == 0)) ? C - 1 - k : k;
                 ap.v_begin = cstart[col];
                 ap.v_end = cstart[col + 1];
                 if (ap.v_end <= ap.v_begin) continue;
                 void (*fn)(vbd::AdjParams) = nullptr;
-                switch (L * 4 + (compact ? 2 : 0)) {
+                switch (L * 4 + alay) {
                     case 16: fn = &vbd::k_adj_sweep<4, 0>; break;
                     case 18: fn = &vbd::k_adj_sweep<4, 2>; break;
+                    case 19: fn = &vbd::k_adj_sweep<4, 3>; break;
                     case 32: fn = &vbd::k_adj_sweep<8, 0>; break;
                     case 34: fn = &vbd::k_adj_sweep<8, 2>; break;
+                    case 35: fn = &vbd::k_adj_sweep<8, 3>; break;
                     case 64: fn = &vbd::k_adj_sweep<16, 0>; break;
                     case 66: fn = &vbd::k_adj_sweep<16, 2>; break;
+                    case 67: fn = &vbd::k_adj_sweep<16, 3>; break;
                     case 128: fn = &vbd::k_adj_sweep<32, 0>; break;
-                    default: fn = &vbd::k_adj_sweep<32, 2>; break;
+                    case 130: fn = &vbd::k_adj_sweep<32, 2>; break;
+                    default: fn = &vbd::k_adj_sweep<32, 3>; break;
                 }
                 cudaLaunchConfig_t cfg = {};
                 cfg.gridDim = dim3(vbd::nblk((long long)(ap.v_end - ap.v_begin) * L, 128));
@@ -450,7 +460,7 @@ struct vbd_solver {
         if (N > nfree) {
             vbd::AdjParams ap{X,      lam,     adj_G.p, y.p,  inc_off.p, inc_tet.p, rec.p,
                               crec.p, cmat.p,  t.dtsr,  nfree, N,        nullptr,   nullptr,
-                              1.0f,   0,       0};
+                              1.0f,   0,       0, cam.p};
             const unsigned grid = vbd::nblk((long long)(N - nfree) * 8, 256);
             vbd::k_adj_pinned<8><<<grid, 256, 0, stream>>>(ap, adj_ax.p);
             VBD_TRY(check_launch());
@@ -548,10 +558,17 @@ struct vbd_solver {
             drop_graphs();
             irec.release();
         }
-        if (layout != 2 && crec.p) {
+        if (layout != 2 && cmat.p) {
+            drop_graphs();
+            cmat.release();
+        }
+        if (layout != 3 && cam.p) {
+            drop_graphs();
+            cam.release();
+        }
+        if (layout != 2 && layout != 3 && crec.p) {
             drop_graphs();
             crec.release();
-            cmat.release();
         }
         if (layout == 1) {
             if (irec.n != (size_t)ninc) {
@@ -562,15 +579,26 @@ struct vbd_solver {
                 vbd::k_pack_stream<<<vbd::nblk(ninc, 256), 256, 0, stream>>>(rec.p, inc_tet.p, irec.p, (int)ninc);
                 VBD_TRY(check_launch());
             }
-        } else if (layout == 2) {
+        } else if (layout == 2 || layout == 3) {
             if (crec.n != 3 * (size_t)ninc) {
                 drop_graphs();
                 VBD_TRY(crec.alloc(3 * (size_t)ninc));
+            }
+            if (layout == 2 && cmat.n != (size_t)ninc) {
+                drop_graphs();
                 VBD_TRY(cmat.alloc(ninc));
             }
-            if (ninc > 0) {
+            if (layout == 3 && cam.n != (size_t)ninc) {
+                drop_graphs();
+                VBD_TRY(cam.alloc(ninc));
+            }
+            if (ninc > 0 && layout == 2) {
                 vbd::k_pack_compact<<<vbd::nblk(ninc, 256), 256, 0, stream>>>(rec.p, inc_tet.p, inc_vertex.p, crec.p,
                                                                              cmat.p, (int)ninc);
+                VBD_TRY(check_launch());
+            } else if (ninc > 0) {
+                vbd::k_pack_factored<<<vbd::nblk(ninc, 256), 256, 0, stream>>>(rec.p, inc_tet.p, inc_vertex.p, crec.p,
+                                                                              cam.p, (int)ninc);
                 VBD_TRY(check_launch());
             }
         }
@@ -698,6 +726,7 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     s->irec.release();
     s->crec.release();
     s->cmat.release();
+    s->cam.release();
 
     // Internal order: free vertices colour by colour (group order), then the pinned ones.
     std::vector<int32_t> perm;
@@ -1150,7 +1179,7 @@ int vbd_solver_energy(vbd_solver* s, int32_t kind, float h, double* out) {
         }
         vbd::SweepParams p{s->x0.p,     nullptr, s->pp.p,    s->y.p, s->inc_off.p, s->inc_tet.p,
                            s->rec.p,    s->irec.p, s->crec.p, s->cmat.p, s->status.p, 0,
-                           s->nfree,    (float)(1.0 / ((double)h * h)), 1.0f};
+                           s->nfree,    (float)(1.0 / ((double)h * h)), 1.0f, 0, 0, s->cam.p};
         const int L = std::max(4, s->lanes);
         const unsigned blocks = vbd::nblk((long long)s->nfree * L, 256);
         switch (L) {
@@ -1218,7 +1247,7 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
             s->block = value;
             return VBD_OK;
         case VBD_OPT_LAYOUT:
-            if (value < 0 || value > 2) VBD_FAIL(VBD_ERR_INVALID_ARG, "layout must be 0, 1 or 2");
+            if (value < 0 || value > 3) VBD_FAIL(VBD_ERR_INVALID_ARG, "layout must be 0, 1, 2 or 3");
             s->layout = value;
             if (s->ready) {
                 VBD_TRY(s->repack_stream());
@@ -1301,9 +1330,9 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
         int lanes, layout, prefetch, pdl, block;
     };
     static const Cand cands[] = {
-        {4, 2, 1, 1, 128}, {8, 2, 1, 1, 128}, {8, 2, 0, 1, 128}, {2, 2, 1, 1, 128}, {16, 2, 1, 1, 128},
-        {4, 2, 1, 0, 128}, {4, 2, 1, 1, 256}, {8, 1, 1, 1, 128}, {4, 1, 1, 1, 128}, {8, 0, 1, 1, 128},
-        {4, 0, 1, 1, 128}, {8, 0, 1, 0, 128},
+        {8, 3, 1, 1, 64}, {8, 3, 1, 1, 128}, {4, 3, 1, 1, 128}, {16, 3, 1, 1, 64}, {8, 3, 0, 1, 64},
+        {8, 3, 1, 0, 64}, {4, 2, 1, 1, 128}, {8, 2, 1, 1, 64},  {2, 2, 1, 1, 128}, {8, 1, 1, 1, 128},
+        {8, 0, 1, 1, 128}, {4, 0, 1, 1, 128},
     };
     const float g[3] = {0.f, 0.f, 0.f};
     cudaEvent_t e0, e1;
