@@ -204,6 +204,18 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
+def wrapper_workload(mesh):
+    """One VBD_GPU_Solver::solveVBD call on the cube as main.cpp issues it: inertial target
+    y = x + N(0, 1e-3 m) on free vertices (seed 7), 1/h^2 = 14400 (h = 1/120), 50 iterations,
+    Chebyshev rho 0.9, starting from x = y."""
+    import numpy as np
+
+    rng = np.random.default_rng(7)
+    y = (mesh.x + 1e-3 * rng.normal(size=mesh.x.shape)).astype(np.float32)
+    y[mesh.fixed == 1] = mesh.x[mesh.fixed == 1]
+    return y, 14400.0, 50, 0.9
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU implementation of the path, timed on the host (rank 0)."""
     from vbd_tetmesh_b200 import meshgen
@@ -236,7 +248,73 @@ def run_reference(args):
         },
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    gpu = reference_gpu_wrapper(mesh)
+    if gpu is not None:
+        line["gpu_wrapper"] = gpu
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_wrapper(mesh):
+    """The reference's own GPU path (VBD_GPU_Solver::solveVBD, its 16-thread-per-vertex kernels)
+    on the wrapper workload, when its library was built (oracle/_ref/libvbdref_gpu.so) and a GPU is
+    present; device time from CUDA events on the stream it launches on."""
+    try:
+        import torch
+
+        if not torch.cuda.is_available():
+            return None
+        from oracle import pyoracle as po
+
+        if not po.ref_gpu_available():
+            return None
+    except ImportError:
+        return None
+    y, dtsr, iters, rho = wrapper_workload(mesh)
+    h = po.RefGpuHandle(mesh, iterations=iters, rho=rho)
+    h.set_inertia(y)
+    h.solve(iters, dtsr, True, rho)
+    ms = sorted(h.solve(iters, dtsr, True, rho) for _ in range(5))
+    h.close()
+    med = ms[len(ms) // 2]
+    return {
+        "workload": "one VBD_GPU_Solver::solveVBD on the cube (y = x + N(0, 1e-3), 1/h^2 14400, 50 iterations, "
+                    "rho 0.9, from x = y): the reference's own kernels",
+        "ms_per_solve": med,
+        "value": mesh.num_verts * iters / (med * 1e-3),
+        "unit": UNIT,
+    }
+
+
+def bench_wrapper(mesh, local, stream):
+    """This project's VBD_OPT_SEMANTICS = 1 path (the reference GPU wrapper's arithmetic, bit-identical
+    to its kernels on this workload in tests/test_gpu_wrapper_mode.py) on the wrapper workload."""
+    import torch
+
+    from vbd_tetmesh_b200 import _capi, build_solver
+
+    y, dtsr, iters, rho = wrapper_workload(mesh)
+    out = {"workload": "one solveVBD on the cube (y = x + N(0, 1e-3), 1/h^2 14400, 50 iterations, rho 0.9, "
+                       "from x = y) with the reference GPU wrapper's semantics"}
+    with torch.cuda.stream(stream):
+        for layout in (0, 1):
+            s = build_solver(mesh, device=local, stream=stream.cuda_stream, layout=layout)
+            s.set_option(_capi.OPT_SEMANTICS, 1)
+            s.update_inertia_from_cpu(y)
+            s.solve_vbd(iters, dtsr, True, rho, _capi.INIT_FROM_INERTIA)
+            s.sync()
+            ms = []
+            for _ in range(5):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                s.solve_vbd(iters, dtsr, True, rho, _capi.INIT_FROM_INERTIA)
+                e1.record(stream)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            s.close()
+            med = sorted(ms)[len(ms) // 2]
+            out[f"layout{layout}"] = {"ms_per_solve": med, "value": mesh.num_verts * iters / (med * 1e-3), "unit": UNIT}
+    return out
 
 
 def bench_batched(args, rank, world, local, stream, dist, barrier):
@@ -577,6 +655,8 @@ def main():
     }
     if clock_info:
         result["clocks"] = clock_info
+    if rank == 0:
+        result["wrapper_semantics"] = bench_wrapper(mesh, local, stream)
     if not args.no_batched:
         result["batched"] = bench_batched(args, rank, world, local, stream, dist, barrier)
     if not args.no_adjoint and rank == 0:

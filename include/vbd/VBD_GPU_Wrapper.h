@@ -1,10 +1,11 @@
 // VBD_GPU_Wrapper.h -- VBD_GPU_Solver with the reference's API (VBD_GPU_Wrapper.h:7-45) over
 // libvbd_b200.  Move-only RAII owner of one vbd_solver handle.
 //
-// solveVBD keeps the wrapper's call shape and its x = y initial guess (VBD_GPU_Wrapper.cu:334) with
-// the Chebyshev blend; the element is the CPU solver's Neo-Hookean model (Energy.cpp:90-158), not the
-// wrapper kernel's corotated stand-in (VBD_GPU_Wrapper.cu:181), and no 1.000001 diagonal factor is
-// added.  Failures throw std::runtime_error with the library's message.
+// The handle runs the wrapper's own semantics (VBD_OPT_SEMANTICS = 1): the corotated element of
+// computeTetContributionLocalCorotated (VBD_DeviceMath.cuh:127-198), the 1.000001 inertia diagonal,
+// solve3x3's guard, float Chebyshev weights, and solveVBD's x = y initial guess
+// (VBD_GPU_Wrapper.cu:332-362).  setSemantics(0) switches to the CPU solver's Neo-Hookean update
+// (Energy.cpp:90-158) instead.  Failures throw std::runtime_error with the library's message.
 #pragma once
 
 #include <utility>
@@ -54,7 +55,14 @@ class VBD_GPU_Solver {
                                  (int32_t)vertexColors.size(), offs.data(), verts.data(), dm.data(), tetRestVol.data(),
                                  nullptr, nullptr),
                  "vbd_solver_init");
+        vbdCheck(vbd_solver_set_option(s_, VBD_OPT_SEMANTICS, semantics_), "vbd_solver_set_option");
         mu_ = lambda_ = -1.0f;
+    }
+
+    // 1 (default) = the reference GPU wrapper's semantics, 0 = VBDsolver's (not in the reference API).
+    void setSemantics(int semantics) {
+        semantics_ = semantics;
+        if (s_) vbdCheck(vbd_solver_set_option(s_, VBD_OPT_SEMANTICS, semantics_), "vbd_solver_set_option");
     }
 
     // One sweep over all colours (VBD_GPU_Wrapper.cu:317-329).
@@ -94,9 +102,11 @@ class VBD_GPU_Solver {
         std::swap(s_, o.s_);
         std::swap(mu_, o.mu_);
         std::swap(lambda_, o.lambda_);
+        std::swap(semantics_, o.semantics_);
     }
     vbd_solver* s_ = nullptr;
     Real mu_ = -1.0f, lambda_ = -1.0f;
+    int semantics_ = 1;
 };
 
 }  // namespace VBD

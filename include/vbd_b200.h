@@ -214,7 +214,9 @@ int vbd_solver_energy(vbd_solver* s, int32_t kind, float h, double* out);
 int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite, int32_t reset);
 
 /* Tuning knobs (all have measured defaults).
- *   VBD_OPT_LANES:       threads cooperating on one vertex: 1, 2, 4, 8, 16 or 32
+ *   VBD_OPT_LANES:       threads cooperating on one vertex: 1, 2, 4, 8, 16 or 32.  Until it is
+ *                        set, vbd_solver_init picks 8 when the free vertices average at least 21
+ *                        incident tets, else 4
  *   VBD_OPT_LAYOUT:      0 = tet records gathered through a per-vertex tet list,
  *                        1 = 64 B tet records copied into incidence order and streamed,
  *                        2 = compact 56 B incidence records streamed (other three vertex ids, their
@@ -223,7 +225,8 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *                            s = M q_n, w = cof(M) q_n, det M for M = their rows of Ps Dm^-1, and the
  *                            material products): the element block without forming F or cof(F);
  *                            the default
- *                        Defaults: 8 lanes, layout 3, 64-thread blocks, prefetch, PDL, graphs.
+ *                        Defaults: layout 3, 64-thread blocks, prefetch, PDL, graphs; lanes
+ *                        chosen by vbd_solver_init (below).
  *   VBD_OPT_GRAPH:       1 = replay a captured CUDA graph per step, 0 = direct launches
  *   VBD_OPT_KERNEL_TIMING: 1 = launch directly and bracket every colour-sweep kernel with a CUDA
  *                        event pair on the handle's stream (read with vbd_solver_kernel_time)
@@ -235,7 +238,18 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *                        with a grid barrier after each one (bounded wait: a barrier that gives up
  *                        makes the next vbd_solver_sync return VBD_ERR_TIMEOUT)
  *   VBD_OPT_ADJOINT_ALTERNATE: 1 = adjoint sweeps alternate the colour order (a forward and a
- *                        backward sweep form one symmetric Gauss-Seidel pair) */
+ *                        backward sweep form one symmetric Gauss-Seidel pair)
+ *   VBD_OPT_SEMANTICS:   0 = the CPU solver's (VBDsolver, VBD.cpp:114-256): Neo-Hookean element,
+ *                        Chebyshev weights with double literals (the default);
+ *                        1 = the reference's GPU wrapper's (VBD_GPU_Solver, VBD_GPU_Wrapper.cu:114-362,
+ *                        VBD_DeviceMath.cuh:127-198): corotated element (5 Higham polar steps,
+ *                        P = 2 mu (F - R) + lambda tr(R^T F - I) R, Hessian 2 mu |q|^2 I +
+ *                        lambda (R q)(R q)^T), inertia diagonal x 1.000001, solve3x3 guard, float
+ *                        Chebyshev weights, 16 lanes per vertex with the wrapper's summation order,
+ *                        tet records read through the per-vertex tet list (any layout), and
+ *                        vbd_solver_step starting each sub-step from x = y as main.cpp's GPU loop
+ *                        does.  Not with VBD_OPT_PERSISTENT, vbd_solver_record or the adjoint;
+ *                        energies and residuals stay the Neo-Hookean ones */
 typedef enum vbd_option {
     VBD_OPT_LANES = 0,
     VBD_OPT_LAYOUT = 1,
@@ -245,7 +259,8 @@ typedef enum vbd_option {
     VBD_OPT_PDL = 5,
     VBD_OPT_BLOCK = 6,
     VBD_OPT_PERSISTENT = 7,
-    VBD_OPT_ADJOINT_ALTERNATE = 8
+    VBD_OPT_ADJOINT_ALTERNATE = 8,
+    VBD_OPT_SEMANTICS = 9
 } vbd_option;
 int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value);
 int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value);

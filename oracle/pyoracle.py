@@ -16,7 +16,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libvbd_oracle.so")
 _lib = None
 
-LITERAL, LITERAL_FULL12, CLOSED = 0, 1, 2
+LITERAL, LITERAL_FULL12, CLOSED, WRAPPER = 0, 1, 2, 3
 
 _p = C.c_void_p
 _i = C.c_int
@@ -308,6 +308,99 @@ class RefHandle:
     def close(self):
         if self._h:
             ref_lib().ref_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+# ---- the reference's GPU wrapper (VBD_GPU_Solver), built by `make -C oracle refgpu` -------------
+# Runs the reference's own kernels on a GPU; used to pin the wrapper-semantics restatement and to
+# time the reference's GPU path.  Available only where oracle/_ref/libvbdref_gpu.so was built and
+# a GPU is present.
+REF_GPU_LIB_PATH = os.path.join(_HERE, "_ref", "libvbdref_gpu.so")
+_ref_gpu_lib = None
+
+
+def ref_gpu_available():
+    return os.path.exists(REF_GPU_LIB_PATH)
+
+
+def ref_gpu_lib():
+    global _ref_gpu_lib
+    if _ref_gpu_lib is None:
+        L = C.CDLL(REF_GPU_LIB_PATH)
+        f = C.c_float
+        L.refgpu_create.argtypes = [_i, _i, _p, _p, _p, _p, f, f, f, f, _i, _i, _p, _i, f]
+        L.refgpu_create.restype = _p
+        L.refgpu_set_inertia.argtypes = [_p, _p]
+        L.refgpu_set_inertia.restype = _i
+        L.refgpu_solve.argtypes = [_p, _i, f, f, f, _i, f, _p]
+        L.refgpu_solve.restype = _i
+        L.refgpu_frame.argtypes = [_p, f, f]
+        L.refgpu_frame.restype = _i
+        L.refgpu_positions.argtypes = [_p, _p]
+        L.refgpu_positions.restype = _i
+        L.refgpu_velocities.argtypes = [_p, _p]
+        L.refgpu_velocities.restype = None
+        L.refgpu_destroy.argtypes = [_p]
+        L.refgpu_destroy.restype = None
+        _ref_gpu_lib = L
+    return _ref_gpu_lib
+
+
+class RefGpuHandle:
+    """The reference's TetMesh + VBDsolver (colouring, Dm^-1, V0) + VBD_GPU_Solver on cuda:0, with
+    scalar mu / lambda as main.cpp passes them."""
+
+    def __init__(self, mesh, dt=1.0 / 60.0, iterations=20, gravity=(0.0, -9.8, 0.0), use_acceleration=True,
+                 rho=0.95, substeps=1):
+        f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)  # noqa: E731
+        self._keep = [f32(mesh.rest).reshape(-1, 3), f32(mesh.x).reshape(-1, 3),
+                      np.ascontiguousarray(mesh.tets, dtype=np.int32), np.ascontiguousarray(mesh.fixed, np.uint8),
+                      f32(gravity)]
+        r, x, t, fx, g = self._keep
+        self.n = r.shape[0]
+        self.mu, self.lam = float(mesh.mu[0]), float(mesh.lam[0])
+        self._h = ref_gpu_lib().refgpu_create(self.n, t.shape[0], _ptr(r), _ptr(x), _ptr(t), _ptr(fx),
+                                              float(mesh.density), self.mu, self.lam, float(dt), int(substeps),
+                                              int(iterations), _ptr(g), int(bool(use_acceleration)), float(rho))
+        if not self._h:
+            raise RuntimeError("the reference's VBD_GPU_Solver could not be set up")
+
+    def set_inertia(self, y):
+        y = np.ascontiguousarray(y, dtype=np.float32).reshape(-1, 3)
+        if ref_gpu_lib().refgpu_set_inertia(self._h, _ptr(y)):
+            raise RuntimeError("CUDA error in the reference's updateInertiaFromCPU")
+
+    def solve(self, iterations, dt_sqr_reciprocal, use_acceleration=True, rho=0.99):
+        """VBD_GPU_Solver::solveVBD; returns its device time in ms."""
+        ms = C.c_float(0.0)
+        if ref_gpu_lib().refgpu_solve(self._h, int(iterations), float(dt_sqr_reciprocal), self.mu, self.lam,
+                                      int(bool(use_acceleration)), float(rho), C.byref(ms)):
+            raise RuntimeError("CUDA error in the reference's solveVBD")
+        return ms.value
+
+    def frame(self, n=1):
+        """n frames of main.cpp's GPU loop."""
+        for _ in range(n):
+            if ref_gpu_lib().refgpu_frame(self._h, self.mu, self.lam):
+                raise RuntimeError("CUDA error in the reference's GPU loop")
+
+    def positions(self):
+        x = np.empty((self.n, 3), np.float32)
+        if ref_gpu_lib().refgpu_positions(self._h, _ptr(x)):
+            raise RuntimeError("CUDA error in the reference's copyPositionsToCPU")
+        return x
+
+    def velocities(self):
+        v = np.empty((self.n, 3), np.float32)
+        ref_gpu_lib().refgpu_velocities(self._h, _ptr(v))
+        return v
+
+    def close(self):
+        if self._h:
+            ref_gpu_lib().refgpu_destroy(self._h)
             self._h = None
 
     def __del__(self):

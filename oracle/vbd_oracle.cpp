@@ -278,7 +278,66 @@ static void tet_block_closed(const M3<T>& DmInv, const M3<T>& F, T lambda, T mu,
             Hn[i][j] = volume * ((i == j ? mu * qq : T(0)) + lambda * Cq[i] * Cq[j]);
 }
 
-enum Mode { LITERAL = 0, LITERAL_FULL12 = 1, CLOSED = 2 };
+// WRAPPER: the semantics of the reference's GPU wrapper (VBD_GPU_Solver) instead of VBDsolver's.
+enum Mode { LITERAL = 0, LITERAL_FULL12 = 1, CLOSED = 2, WRAPPER = 3 };
+
+// ---- VBD_GPU_Solver semantics (VBD_GPU_Wrapper.cu:114-235, 332-362; VBD_DeviceMath.cuh) ----------
+
+// det3x3 of VBD_DeviceMath.cuh:11-15 (expansion along row 0).
+template <class T> static inline T det3_row0(const T A[3][3]) {
+    return A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) - A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+           A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+}
+
+template <class T> static inline void cof3(const T F[3][3], T C[3][3]) {
+    C[0][0] = F[1][1] * F[2][2] - F[1][2] * F[2][1];
+    C[0][1] = F[1][2] * F[2][0] - F[1][0] * F[2][2];
+    C[0][2] = F[1][0] * F[2][1] - F[1][1] * F[2][0];
+    C[1][0] = F[2][1] * F[0][2] - F[2][2] * F[0][1];
+    C[1][1] = F[2][2] * F[0][0] - F[2][0] * F[0][2];
+    C[1][2] = F[2][0] * F[0][1] - F[2][1] * F[0][0];
+    C[2][0] = F[0][1] * F[1][2] - F[0][2] * F[1][1];
+    C[2][1] = F[0][2] * F[1][0] - F[0][0] * F[1][2];
+    C[2][2] = F[0][0] * F[1][1] - F[0][1] * F[1][0];
+}
+
+// computeTetContributionLocalCorotated (VBD_DeviceMath.cuh:127-198): polar factor R of F by five
+// Higham steps R <- (R + cof(R)/det R)/2 (stopping when |det R| < 1e-8), tr = R:F - 3,
+// P = 2 mu (F - R) + lambda tr R, g = V P q_n, H = V (2 mu |q_n|^2 I + lambda (R q_n)(R q_n)^T).
+template <class T>
+static void corot_block(const M3<T>& Di, const M3<T>& Fm, T mu, T lambda, T volume, int n, T H[9], T g[3]) {
+    T F[3][3], R[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) R[a][b] = F[a][b] = Fm.m[a][b];
+    for (int it = 0; it < 5; ++it) {
+        T det = det3_row0(R);
+        if (std::abs(double(det)) < 1e-8) break;
+        T C[3][3];
+        cof3(R, C);
+        T inv = T(1) / det;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) R[a][b] = T(0.5) * (R[a][b] + C[a][b] * inv);
+    }
+    T tr = T(0);
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) tr += R[a][b] * F[a][b];
+    tr -= T(3);
+    T P[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) P[a][b] = T(2) * mu * (F[a][b] - R[a][b]) + lambda * tr * R[a][b];
+    T q[3];
+    if (n == 0) {
+        for (int c = 0; c < 3; ++c) q[c] = -Di.m[0][c] - Di.m[1][c] - Di.m[2][c];
+    } else {
+        for (int c = 0; c < 3; ++c) q[c] = Di.m[n - 1][c];
+    }
+    for (int a = 0; a < 3; ++a) g[a] = volume * (P[a][0] * q[0] + P[a][1] * q[1] + P[a][2] * q[2]);
+    T qsq = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+    T RQ[3];
+    for (int a = 0; a < 3; ++a) RQ[a] = R[a][0] * q[0] + R[a][1] * q[1] + R[a][2] * q[2];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) H[3 * a + b] = volume * ((a == b ? T(2) * mu * qsq : T(0)) + lambda * RQ[a] * RQ[b]);
+}
 
 template <class T> struct Sim {
     int N = 0, NT = 0;
@@ -366,7 +425,52 @@ template <class T> struct Sim {
     }
 
     // VBDsolver::solveVertex + the update in VBDsolver::solve (VBD.cpp:124-156, 160-203).
+    // vbd_solve_color_kernel (VBD_GPU_Wrapper.cu:114-235) for one vertex: 16 partial sums (thread t
+    // of the block takes incident tets t, t + 16, ...), added in thread order onto
+    // H = m/h^2 * 1.000001 I and f = m/h^2 (y - x); solve3x3 (VBD_DeviceMath.cuh:47-64).
+    void solve_vertex_wrapper(int vid, T dtSqrRecip) {
+        constexpr int kThreads = 16;
+        T hs[kThreads][9] = {}, fs[kThreads][3] = {};
+        for (int a = adj_off[vid]; a < adj_off[vid + 1]; ++a) {
+            const int lane = (a - adj_off[vid]) % kThreads;
+            int t = adj[a];
+            const int32_t* tet = &tets[4 * t];
+            int n = -1;
+            for (int i = 0; i < 4; ++i)
+                if (tet[i] == vid) {
+                    n = i;
+                    break;
+                }
+            if (n < 0) continue;
+            M3<T> Ds = edge_matrix(x.data(), tet);
+            M3<T> F = matmul(Ds, DmInv[t]);
+            T Hl[9], gl[3];
+            corot_block(DmInv[t], F, mu[t], lam[t], V0[t], n, Hl, gl);
+            for (int k = 0; k < 9; ++k) hs[lane][k] += Hl[k];
+            for (int k = 0; k < 3; ++k) fs[lane][k] -= gl[k];
+        }
+        T coeff = mass[vid] * dtSqrRecip;
+        T reg = coeff * T(1.000001f);
+        T H[3][3] = {{reg, T(0), T(0)}, {T(0), reg, T(0)}, {T(0), T(0), reg}};
+        T f[3];
+        for (int c = 0; c < 3; ++c) f[c] = coeff * (y[3 * vid + c] - x[3 * vid + c]);
+        for (int l = 0; l < kThreads; ++l) {
+            for (int k = 0; k < 9; ++k) H[k / 3][k % 3] += hs[l][k];
+            for (int k = 0; k < 3; ++k) f[k] += fs[l][k];
+        }
+        T det = det3_row0(H);
+        if (std::abs(double(det)) < 1e-8) return;
+        T adjm[3][3];
+        cof3(H, adjm);
+        T inv = T(1) / det;
+        for (int i = 0; i < 3; ++i) x[3 * vid + i] += inv * (adjm[0][i] * f[0] + adjm[1][i] * f[1] + adjm[2][i] * f[2]);
+    }
+
     void solve_vertex(int vid, T dtSqrRecip) {
+        if (mode == WRAPPER) {
+            solve_vertex_wrapper(vid, dtSqrRecip);
+            return;
+        }
         T H[3][3] = {};
         T f[3];
         T m = mass[vid];
@@ -438,6 +542,13 @@ template <class T> struct Sim {
         }
     }
 
+    // getAcceleratorOmega of the GPU wrapper (VBD_GPU_Wrapper.cu:240-244): arithmetic in T.
+    static T omega_of_wrapper(int order, T rho, T prev) {
+        if (order == 1) return T(1);
+        if (order == 2) return T(2) / (T(2) - (rho * rho));
+        return T(4) / (T(4) - (rho * rho) * prev);
+    }
+
     // getAcceleratorOmega (VBD.cpp:302-311), with the reference's double literals.
     static T omega_of(int order, T rho, T prev) {
         if (order == 1) return T(1);
@@ -476,7 +587,7 @@ template <class T> struct Sim {
             std::vector<T> cur = x;
             sweep(dtSqrRecip);
             if (accel) {
-                omega = omega_of(it + 1, rho, omega);
+                omega = mode == WRAPPER ? omega_of_wrapper(it + 1, rho, omega) : omega_of(it + 1, rho, omega);
                 if (omega > T(1)) {
                     for (int i = 0; i < N; ++i) {
                         if (fixed[i]) continue;
@@ -505,6 +616,12 @@ template <class T> struct Sim {
                 for (int c = 0; c < 3; ++c)
                     y[3 * i + c] = fixed[i] ? x[3 * i + c] : x[3 * i + c] + subDt * v[3 * i + c];
             T dtSqrRecip = T(1.0 / double(subDt * subDt));
+            // main.cpp's GPU loop: solveVBD starts from x = y and takes 1/subDt^2 in float
+            // (main.cpp:211-225, VBD_GPU_Wrapper.cu:334)
+            if (mode == WRAPPER) {
+                x = y;
+                dtSqrRecip = T(1) / (subDt * subDt);
+            }
             solve_loop(dtSqrRecip, iters, accel, rho, ehist);
             // updateVelocity (TetMesh.h:305-311)
             for (int i = 0; i < N; ++i) {
@@ -892,7 +1009,8 @@ void orc_mesh_setup(int precision, int N, int NT, const double* rest, const int3
         run(orc::Sim<float>());
 }
 
-// Runs nsteps of VBDsolver::step.  mode: 0 literal block, 1 literal full 12x12, 2 closed form.
+// Runs nsteps of VBDsolver::step.  mode: 0 literal block, 1 literal full 12x12, 2 closed form,
+// 3 the GPU wrapper's semantics (corotated element; each substep as main.cpp's GPU loop runs it).
 // ip_out[nsteps] (nullable): incremental potential after each step; ehist_out (nullable):
 // computeTotalEnergy every 10 iterations, nsteps*substeps*ceil(iters/10) values.
 int orc_simulate(int precision, int mode, int threads, int N, int NT, const double* rest, const double* x0,
@@ -962,7 +1080,11 @@ void orc_tet_block(int precision, int mode, const double* F9, const double* dmin
                 D.m[a][b] = T(dminv9[3 * a + b]);
             }
         T H[3][3], g[3];
-        if (mode == orc::CLOSED)
+        if (mode == orc::WRAPPER) {
+            T Hf[9];
+            orc::corot_block(D, F, T(mu), T(lambda), T(vol), n, Hf, g);
+            for (int k = 0; k < 9; ++k) H[k / 3][k % 3] = Hf[k];
+        } else if (mode == orc::CLOSED)
             orc::tet_block_closed(D, F, T(lambda), T(mu), T(vol), n, H, g);
         else
             orc::tet_block_literal(D, F, T(lambda), T(mu), T(vol), n, H, g, mode == orc::LITERAL_FULL12);

@@ -41,8 +41,9 @@ def run_cpp(m, iters, steps, dt, rho, tmp_path):
 
 
 def wrapper_flow_oracle(m, iters, steps, dt, rho):
-    """The main.cpp loop: host predictor (float32, TetMesh.h:319-348), solve from x = y
-    (VBD_GPU_Wrapper.cu:334) by the oracle, host velocity update (TetMesh.h:305-311)."""
+    """The main.cpp loop: host predictor (float32, TetMesh.h:319-348), solveVBD from x = y with the
+    GPU wrapper's semantics (VBD_GPU_Wrapper.cu:332-362) by the oracle, host velocity update
+    (TetMesh.h:305-311)."""
     dt32 = np.float32(dt)
     dtsr = np.float32(1.0) / (dt32 * dt32)
     x = m.x.astype(np.float32).copy()
@@ -54,7 +55,8 @@ def wrapper_flow_oracle(m, iters, steps, dt, rho):
         v[free] = v[free] + dt32 * g
         y = x.copy()
         y[free] = x[free] + dt32 * v[free]
-        x = po.solve(m, x, y, float(dtsr), iters, True, rho, init_from_inertia=True).astype(np.float32)
+        x = po.solve(m, x, y, float(dtsr), iters, True, rho, init_from_inertia=True,
+                     mode=po.WRAPPER).astype(np.float32)
         v[free] = ((x[free] - xprev[free]) / dt32) * np.float32(0.999)
     return x
 

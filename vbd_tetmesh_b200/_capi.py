@@ -37,6 +37,9 @@ OPT_PDL = 5
 OPT_BLOCK = 6
 OPT_PERSISTENT = 7
 OPT_ADJOINT_ALTERNATE = 8
+OPT_SEMANTICS = 9
+SEMANTICS_VBDSOLVER = 0
+SEMANTICS_GPU_WRAPPER = 1
 
 _p = C.c_void_p
 _i32 = C.c_int32

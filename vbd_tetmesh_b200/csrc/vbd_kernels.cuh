@@ -487,6 +487,193 @@ __global__ void __launch_bounds__(256) k_sweep(SweepParams p) {
     vertex_update<LANES, LAYOUT, PREFETCH, false>(p, v, lane, active, j, j1, nxt);
 }
 
+// ---- VBD_GPU_Solver semantics (the reference's GPU wrapper) ------------------------------------
+//
+// The element and vertex update of vbd_solve_color_kernel (VBD_GPU_Wrapper.cu:114-235) with
+// computeTetContributionLocalCorotated (VBD_DeviceMath.cuh:127-198), in that code's arithmetic:
+//   F = Ds Dm^-1 (Ds columns x_k - x_0), R by 5 Higham steps R <- (R + cof(R)/det R)/2 that stop
+//   when |det R| < 1e-8, tr = R:F - 3, P = 2 mu (F - R) + lambda tr R, g = V P q_n,
+//   H = V (2 mu |q_n|^2 I + lambda (R q_n)(R q_n)^T);
+// 16 lanes per vertex, lane t summing tets t, t + 16, ... (H += H_e, f -= g_e), then the 16
+// partial sums added in lane order onto H = m/h^2 * 1.000001 I, f = m/h^2 (y - x), and the 3x3
+// solve of solve3x3 (VBD_DeviceMath.cuh:47-64: row-0 determinant, skip when |det| < 1e-8).
+// The Chebyshev blend is the reference's post-sweep kernel (VBD_GPU_Wrapper.cu:8-20) folded into
+// the sweep exactly as for the default semantics.
+
+__device__ __forceinline__ float det3_row0(const float A[3][3]) {
+    return A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) - A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+           A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+}
+
+__device__ __forceinline__ void cofactor3(const float F[3][3], float C[3][3]) {
+    C[0][0] = F[1][1] * F[2][2] - F[1][2] * F[2][1];
+    C[0][1] = F[1][2] * F[2][0] - F[1][0] * F[2][2];
+    C[0][2] = F[1][0] * F[2][1] - F[1][1] * F[2][0];
+    C[1][0] = F[2][1] * F[0][2] - F[2][2] * F[0][1];
+    C[1][1] = F[2][2] * F[0][0] - F[2][0] * F[0][2];
+    C[1][2] = F[2][0] * F[0][1] - F[2][1] * F[0][0];
+    C[2][0] = F[0][1] * F[1][2] - F[0][2] * F[1][1];
+    C[2][1] = F[0][2] * F[1][0] - F[0][0] * F[1][2];
+    C[2][2] = F[0][0] * F[1][1] - F[0][1] * F[1][0];
+}
+
+// Corotated block of tet r at vertex v (internal id); false when v is not one of its vertices.
+__device__ __forceinline__ bool corot_block(const TetRec& r, int v, float4 xi, const float4* __restrict__ X,
+                                            float H[9], float g[3]) {
+    const int ids[4] = {r.ids.x, r.ids.y, r.ids.z, r.ids.w};
+    const int n = (ids[0] == v) ? 0 : (ids[1] == v) ? 1 : (ids[2] == v) ? 2 : (ids[3] == v) ? 3 : -1;
+    if (n < 0) return false;
+    float4 pos[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) pos[k] = (ids[k] == v) ? xi : X[ids[k]];
+    const float Di[3][3] = {{r.a.x, r.a.y, r.a.z}, {r.a.w, r.b.x, r.b.y}, {r.b.z, r.b.w, r.c.x}};
+    const float Ds[3][3] = {{pos[1].x - pos[0].x, pos[2].x - pos[0].x, pos[3].x - pos[0].x},
+                            {pos[1].y - pos[0].y, pos[2].y - pos[0].y, pos[3].y - pos[0].y},
+                            {pos[1].z - pos[0].z, pos[2].z - pos[0].z, pos[3].z - pos[0].z}};
+    float F[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) F[a][b] = Ds[a][0] * Di[0][b] + Ds[a][1] * Di[1][b] + Ds[a][2] * Di[2][b];
+    float R[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) R[a][b] = F[a][b];
+    for (int it = 0; it < 5; ++it) {
+        const float det = det3_row0(R);
+        if (fabsf(det) < 1e-8f) break;
+        float C[3][3];
+        cofactor3(R, C);
+        const float inv = 1.0f / det;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) R[a][b] = 0.5f * (R[a][b] + C[a][b] * inv);
+    }
+    float tr = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) tr += R[a][b] * F[a][b];
+    tr -= 3.0f;
+    const float mu = r.c.z, lam = r.c.w, vol = r.c.y;
+    float P[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) P[a][b] = 2.0f * mu * (F[a][b] - R[a][b]) + lam * tr * R[a][b];
+    float q[3];
+    if (n == 0) {
+        q[0] = -Di[0][0] - Di[1][0] - Di[2][0];
+        q[1] = -Di[0][1] - Di[1][1] - Di[2][1];
+        q[2] = -Di[0][2] - Di[1][2] - Di[2][2];
+    } else {
+        q[0] = Di[n - 1][0];
+        q[1] = Di[n - 1][1];
+        q[2] = Di[n - 1][2];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) g[a] = vol * (P[a][0] * q[0] + P[a][1] * q[1] + P[a][2] * q[2]);
+    const float qsq = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+    float RQ[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) RQ[a] = R[a][0] * q[0] + R[a][1] * q[1] + R[a][2] * q[2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) H[3 * a + b] = vol * ((a == b ? 2.0f * mu * qsq : 0.0f) + lam * RQ[a] * RQ[b]);
+    return true;
+}
+
+constexpr int kWrapperLanes = 16;
+
+// Tet records are read through the per-vertex tet list whatever the layout option, as the
+// reference's kernel reads them; this one code path is the one checked bit for bit against it.
+__global__ void __launch_bounds__(256) k_sweep_wrapper(SweepParams p) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & (kWrapperLanes - 1);
+    const int v = p.v_begin + t / kWrapperLanes;
+    const bool active = v < p.v_end;
+    int j0 = 0, j1 = 0;
+    if (active) {
+        j0 = __ldg(p.inc_off + v);
+        j1 = __ldg(p.inc_off + v + 1);
+    }
+    int j = j0 + lane;
+    TetRec nxt;
+    if (j < j1) nxt = Elem<0>::fetch(p, j);
+    pdl_trigger();
+    pdl_wait();
+    const float4 xi = active ? p.x[v] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float hs[9], fs[3];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) hs[k] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) fs[k] = 0.0f;
+    for (; j < j1; j += kWrapperLanes) {
+        const TetRec r = nxt;
+        if (j + kWrapperLanes < j1) nxt = Elem<0>::fetch(p, j + kWrapperLanes);
+        float H[9], g[3];
+        if (corot_block(r, v, xi, p.x, H, g)) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) hs[k] += H[k];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) fs[k] -= g[k];
+        }
+    }
+    // partial sums added in lane order by the group's first lane
+    float Hf[9], ff[3];
+    if (lane == 0 && active) {
+        const float4 yi = p.y[v];
+        const float coeff = yi.w * p.dtsr;
+        const float reg = coeff * 1.000001f;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Hf[k] = (k % 4 == 0) ? reg : 0.0f;
+        ff[0] = coeff * (yi.x - xi.x);
+        ff[1] = coeff * (yi.y - xi.y);
+        ff[2] = coeff * (yi.z - xi.z);
+    }
+    for (int src = 0; src < kWrapperLanes; ++src) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const float o = __shfl_sync(0xffffffffu, hs[k], src, kWrapperLanes);
+            if (lane == 0) Hf[k] += o;
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float o = __shfl_sync(0xffffffffu, fs[k], src, kWrapperLanes);
+            if (lane == 0) ff[k] += o;
+        }
+    }
+    if (!active || lane != 0) return;
+    const float A[3][3] = {{Hf[0], Hf[1], Hf[2]}, {Hf[3], Hf[4], Hf[5]}, {Hf[6], Hf[7], Hf[8]}};
+    const float det = det3_row0(A);
+    float4 xn = xi;
+    if (fabsf(det) < 1.0e-8f) {
+        atomicAdd(p.status + ST_SINGULAR, 1ull);
+    } else {
+        float adj[3][3];
+        cofactor3(A, adj);
+        const float inv = 1.0f / det;
+        xn.x = xi.x + inv * (adj[0][0] * ff[0] + adj[1][0] * ff[1] + adj[2][0] * ff[2]);
+        xn.y = xi.y + inv * (adj[0][1] * ff[0] + adj[1][1] * ff[1] + adj[2][1] * ff[2]);
+        xn.z = xi.z + inv * (adj[0][2] * ff[0] + adj[1][2] * ff[1] + adj[2][2] * ff[2]);
+    }
+    if (!(isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z))) p.status[ST_NONFINITE] = 1ull;
+    p.x[v] = xn;
+    if (p.accel) {
+        const float4 q = p.pp[v];
+        float4 xa;
+        xa.x = p.omega * (xn.x - q.x) + q.x;
+        xa.y = p.omega * (xn.y - q.y) + q.y;
+        xa.z = p.omega * (xn.z - q.z) + q.z;
+        xa.w = xn.w;
+        p.xnext[v] = xa;
+    }
+    if (p.keep_pp) p.pp[v] = xi;
+}
+
 // ---- persistent colour-walking kernel -------------------------------------------------------
 
 struct GridBarrier {
@@ -574,9 +761,9 @@ __global__ void __launch_bounds__(256, 4) k_persistent(PersistParams p) {
                 vi.y += p.hgy;
                 vi.z += p.hgz;
                 p.v[i] = vi;
-                yi.x = xi.x + p.h * vi.x;
-                yi.y = xi.y + p.h * vi.y;
-                yi.z = xi.z + p.h * vi.z;
+                yi.x = __fadd_rn(xi.x, __fmul_rn(p.h, vi.x));
+                yi.y = __fadd_rn(xi.y, __fmul_rn(p.h, vi.y));
+                yi.z = __fadd_rn(xi.z, __fmul_rn(p.h, vi.z));
             } else {
                 yi.x = xi.x;
                 yi.y = xi.y;
@@ -647,6 +834,8 @@ __global__ void __launch_bounds__(256, 4) k_persistent(PersistParams p) {
 
 // Inertial predictor (VBDsolver::forwardStep, VBD.cpp:103-112; TetMesh::applyGravity /
 // computeInertia / savePreviousPosition, TetMesh.h:319-348).  Free vertices are [0, nfree).
+// y = x + h v is rounded after the product and after the sum (no fused multiply-add), as the
+// reference's host code computes it.
 __global__ void k_predict(const float4* __restrict__ x, float4* __restrict__ v, float4* __restrict__ xprev,
                           float4* __restrict__ y, int nfree, int n, float h, float hgx, float hgy, float hgz) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -660,9 +849,9 @@ __global__ void k_predict(const float4* __restrict__ x, float4* __restrict__ v, 
         vi.y += hgy;
         vi.z += hgz;
         v[i] = vi;
-        yi.x = xi.x + h * vi.x;
-        yi.y = xi.y + h * vi.y;
-        yi.z = xi.z + h * vi.z;
+        yi.x = __fadd_rn(xi.x, __fmul_rn(h, vi.x));
+        yi.y = __fadd_rn(xi.y, __fmul_rn(h, vi.y));
+        yi.z = __fadd_rn(xi.z, __fmul_rn(h, vi.z));
     } else {
         yi.x = xi.x;
         yi.y = xi.y;

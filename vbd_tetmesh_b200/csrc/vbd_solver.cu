@@ -58,6 +58,13 @@ static float omega_of(int order, float rho, float prev) {
     return (float)(4.0 / (4.0 - (double)(rho * rho * prev)));
 }
 
+// getAcceleratorOmega of the GPU wrapper (VBD_GPU_Wrapper.cu:240-244): float arithmetic.
+static float omega_of_wrapper(int order, float rho, float prev) {
+    if (order == 1) return 1.0f;
+    if (order == 2) return 2.0f / (2.0f - (rho * rho));
+    return 4.0f / (4.0f - (rho * rho) * prev);
+}
+
 using SweepFn = void (*)(SweepParams);
 
 template <int L> static SweepFn pick_sweep(int layout, bool prefetch) {
@@ -83,7 +90,7 @@ static SweepFn pick_sweep(int lanes, int layout, bool prefetch) {
 // Key of a captured step / solve graph: everything baked into its kernel parameters.
 struct GraphKey {
     int kind;  // 0 = step, 1 = solve, 2 = single sweep
-    int iters, accel, init, lanes, layout, prefetch, pdl, block;
+    int iters, accel, init, lanes, layout, prefetch, pdl, block, semantics;
     float h, dtsr, hg[3], rho;
     bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
 };
@@ -118,6 +125,15 @@ struct vbd_solver {
     // defaults: the fastest shape measured on the 64^3 cube (compact streamed records, 4 lanes per
     // vertex, record prefetch, programmatic dependent launch, 128-thread blocks)
     int lanes = 8, layout = 3, use_graph = 1, timing = 0, prefetch = 1, pdl = 1, block = 64;
+    // Until VBD_OPT_LANES is set, init picks the lane count from the mean number of incident tets
+    // per free vertex: 8 lanes from 21 up (the 64^3 cube: 22.9, 5.09 vs 5.49 ms/step with 4), else 4
+    // (the 512-block batch: 19.5, 9.06 vs 10.2 ms/step with 8).
+    bool lanes_auto = true;
+    // VBD_OPT_SEMANTICS: 0 = VBDsolver (VBD.cpp), 1 = VBD_GPU_Solver (VBD_GPU_Wrapper.cu)
+    int semantics = 0;
+    float omega_next(int k, float rho, float prev) const {
+        return semantics ? vbd::omega_of_wrapper(k, rho, prev) : vbd::omega_of(k, rho, prev);
+    }
     int persistent = 0;                             // whole step in one cooperative launch
     long long spin_limit = 1LL << 22;               // barrier polls before a persistent launch gives up
     vbd::DBuf<int> d_cstart;
@@ -202,8 +218,12 @@ struct vbd_solver {
         vbd::SweepParams p{xr,     xn,     pp.p,     y.p, inc_off.p, inc_tet.p, rec.p,          irec.p,
                            crec.p, cmat.p, status.p, vb,  ve,        dtsr,      omega, accel ? 1 : 0,
                            keep_pp ? 1 : 0, cam.p};
-        const long long threads = (long long)(ve - vb) * lanes;
+        long long threads = (long long)(ve - vb) * lanes;
         vbd::SweepFn fn = vbd::pick_sweep(lanes, layout, prefetch != 0);
+        if (semantics) {
+            threads = (long long)(ve - vb) * vbd::kWrapperLanes;
+            fn = &vbd::k_sweep_wrapper;
+        }
         cudaEvent_t ev[2] = {nullptr, nullptr};
         if (timing) {
             VBD_TRY(timing_event(ev));
@@ -235,7 +255,7 @@ struct vbd_solver {
         for (int k = 1; k <= iters; ++k) {
             bool blend = false;
             if (accel) {
-                omega = vbd::omega_of(k, rho, omega);
+                omega = omega_next(k, rho, omega);
                 blend = omega > 1.0f;
             }
             float4* xr = cur ? x1.p : x0.p;
@@ -250,6 +270,12 @@ struct vbd_solver {
         vbd::k_predict<<<vbd::nblk(N, 256), 256, 0, stream>>>(x0.p, v.p, xprev.p, y.p, nfree, N, h, hg[0], hg[1],
                                                               hg[2]);
         VBD_TRY(check_launch());
+        if (semantics) {
+            // main.cpp's GPU loop: solveVBD starts every substep from the inertial target
+            // (VBD_GPU_Wrapper.cu:334)
+            vbd::k_copy_xyz<<<vbd::nblk(N, 256), 256, 0, stream>>>(y.p, x0.p, x1.p, N);
+            VBD_TRY(check_launch());
+        }
         int cur = 0;
         VBD_TRY(emit_iterations(iters, dtsr, accel, rho, cur));
         if (nfree > 0) {
@@ -279,7 +305,7 @@ struct vbd_solver {
         std::vector<float> w(std::max(iters, 1), 1.0f);
         float omega = 1.0f;
         for (int k = 1; k <= iters; ++k) {
-            if (accel) omega = vbd::omega_of(k, rho, omega);
+            if (accel) omega = omega_next(k, rho, omega);
             w[k - 1] = accel ? omega : 1.0f;
         }
         return w;
@@ -383,6 +409,7 @@ struct vbd_solver {
         key.prefetch = prefetch;
         key.pdl = pdl;
         key.block = block;
+        key.semantics = semantics;
         key.h = t.h;
         key.dtsr = t.dtsr;
         key.hg[0] = t.hg[0];
@@ -809,6 +836,7 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     CUDA_TRY(cudaMemcpy(s->rec.p, rec.data(), sizeof(vbd::TetRec) * rec.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemset(s->status.p, 0, sizeof(unsigned long long) * vbd::ST_SLOTS));
 
+    if (s->lanes_auto) s->lanes = (nfree > 0 && (double)ninc >= 21.0 * nfree) ? 8 : 4;
     s->colour_bytes.assign(num_colours, 0.0);
     for (int c = 0; c < num_colours; ++c)
         for (int i = cstart[c]; i < cstart[c + 1]; ++i)
@@ -978,6 +1006,7 @@ int vbd_solver_solve(vbd_solver* s, int32_t iterations, float dt_sqr_reciprocal,
     key.prefetch = s->prefetch;
     key.pdl = s->pdl;
     key.block = s->block;
+    key.semantics = s->semantics;
     key.dtsr = dt_sqr_reciprocal;
     key.rho = rho;
     if (s->persistent && !s->timing)
@@ -1008,7 +1037,8 @@ int vbd_solver_step(vbd_solver* s, float dt, int32_t substeps, int32_t iteration
     if (!gravity) VBD_FAIL(VBD_ERR_INVALID_ARG, "gravity is null");
     DeviceScope scope(s->device);
     const float h = dt / (float)substeps;
-    const float dtsr = (float)(1.0 / (double)(h * h));
+    // 1/h^2: VBD.cpp computes it through double, main.cpp's GPU loop in float (main.cpp:211)
+    const float dtsr = s->semantics ? 1.0f / (h * h) : (float)(1.0 / (double)(h * h));
     const float hg[3] = {h * gravity[0], h * gravity[1], h * gravity[2]};
     vbd::GraphKey key{};
     key.kind = 0;
@@ -1019,6 +1049,7 @@ int vbd_solver_step(vbd_solver* s, float dt, int32_t substeps, int32_t iteration
     key.prefetch = s->prefetch;
     key.pdl = s->pdl;
     key.block = s->block;
+    key.semantics = s->semantics;
     key.h = h;
     key.dtsr = dtsr;
     key.hg[0] = hg[0];
@@ -1039,6 +1070,8 @@ int vbd_solver_record(vbd_solver* s, int32_t checkpoint_every) {
     vbd::clear_error();
     VBD_TRY(need_ready(s));
     if (checkpoint_every < 0) VBD_FAIL(VBD_ERR_INVALID_ARG, "checkpoint_every must be >= 0");
+    if (checkpoint_every > 0 && s->semantics)
+        VBD_FAIL(VBD_ERR_STATE, "the adjoint differentiates the VBDsolver semantics; set VBD_OPT_SEMANTICS to 0");
     DeviceScope scope(s->device);
     s->tape.clear();
     s->ckpts.clear();
@@ -1228,6 +1261,7 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
             if (value != 1 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)
                 VBD_FAIL(VBD_ERR_INVALID_ARG, "lanes must be 1, 2, 4, 8, 16 or 32");
             s->lanes = value;
+            s->lanes_auto = false;
             return VBD_OK;
         case VBD_OPT_PREFETCH:
             s->prefetch = value ? 1 : 0;
@@ -1236,7 +1270,17 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
             s->pdl = value ? 1 : 0;
             return VBD_OK;
         case VBD_OPT_PERSISTENT:
+            if (value && s->semantics)
+                VBD_FAIL(VBD_ERR_INVALID_ARG, "the persistent kernel runs the VBDsolver semantics only");
             s->persistent = value ? 1 : 0;
+            return VBD_OK;
+        case VBD_OPT_SEMANTICS:
+            if (value != 0 && value != 1) VBD_FAIL(VBD_ERR_INVALID_ARG, "semantics must be 0 (VBDsolver) or 1 (VBD_GPU_Solver)");
+            if (value && s->persistent)
+                VBD_FAIL(VBD_ERR_INVALID_ARG, "the persistent kernel runs the VBDsolver semantics only");
+            if (value && s->ckpt_every > 0)
+                VBD_FAIL(VBD_ERR_STATE, "recording for the adjoint is on; the adjoint needs the VBDsolver semantics");
+            s->semantics = value;
             return VBD_OK;
         case VBD_OPT_ADJOINT_ALTERNATE:
             s->adj_alternate = value ? 1 : 0;
@@ -1277,6 +1321,7 @@ int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value) {
         case VBD_OPT_PDL: *value = s->pdl; return VBD_OK;
         case VBD_OPT_BLOCK: *value = s->block; return VBD_OK;
         case VBD_OPT_PERSISTENT: *value = s->persistent; return VBD_OK;
+        case VBD_OPT_SEMANTICS: *value = s->semantics; return VBD_OK;
         case VBD_OPT_ADJOINT_ALTERNATE: *value = s->adj_alternate; return VBD_OK;
         default: VBD_FAIL(VBD_ERR_INVALID_ARG, "unknown option %d", option);
     }
