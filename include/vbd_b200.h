@@ -74,6 +74,29 @@ int vbd_precompute_tets(int32_t num_verts, int32_t num_tets, const float* rest_x
                         float* dm_inv, float* rest_vol);
 
 /* ------------------------------------------------------------------------------------------
+ * TetGen input and pinning (the reference driver's loadTetgenModel / readNodeFile and its
+ * boundary rule, main.cpp:14-168).  Host only.
+ * ------------------------------------------------------------------------------------------ */
+
+/* Reads a TetGen .node file.  With positions == NULL only *num_nodes is set (the header count);
+ * otherwise `capacity` >= *num_nodes positions are written xyz-interleaved and *first_index (if
+ * not NULL) receives the first node's index: 0 means the mesh's ids are 0-based, else 1-based
+ * (main.cpp:37-38).  Blank lines and '#' comment lines are skipped. */
+int vbd_tetgen_read_node(const char* path, int32_t* num_nodes, int32_t* first_index, float* positions,
+                         int32_t capacity);
+
+/* Reads a TetGen .ele file (four vertex ids per element; index_base 0 or 1 is subtracted,
+ * main.cpp:113-115).  With tets == NULL only *num_tets is set.  Ids must lie in [0, num_nodes)
+ * when num_nodes >= 0. */
+int vbd_tetgen_read_ele(const char* path, int32_t index_base, int32_t num_nodes, int32_t* num_tets, int32_t* tets,
+                        int32_t capacity);
+
+/* Sets fixed[i] = 1 for every vertex whose coordinate `axis` (0 = x, 1 = y, 2 = z) is at most
+ * min + (max - min) * fraction over all vertices, in float arithmetic (main.cpp:127-163 with
+ * fraction 0.05 on y); entries already set stay set. */
+int vbd_pin_low_fraction(int32_t num_verts, const float* positions, int32_t axis, float fraction, uint8_t* fixed);
+
+/* ------------------------------------------------------------------------------------------
  * Solver handle (one GPU).  Replaces VBD::VBD_GPU_Solver (VBD_GPU_Wrapper.h:7-45) and the
  * step loop of VBD::VBDsolver (VBD.cpp:60-112).
  * ------------------------------------------------------------------------------------------ */

@@ -6,7 +6,7 @@ library, or without a B200, the solver calls raise.
 """
 from ._capi import VBDError, lib  # noqa: F401
 from .solver import GPUSolver, build_batch_solver, build_solver, color_vertices, mesh_mass, precompute_tets  # noqa: F401
-from . import meshgen  # noqa: F401
+from . import meshgen, surface, tetgen  # noqa: F401
 
 __all__ = ["VBDError", "lib", "GPUSolver", "build_solver", "build_batch_solver", "color_vertices", "mesh_mass", "precompute_tets",
-           "meshgen"]
+           "meshgen", "surface", "tetgen"]
