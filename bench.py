@@ -325,7 +325,7 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
     balanced by tet count; times are the max over ranks."""
     import torch
 
-    from vbd_tetmesh_b200 import build_batch_solver, build_solver, meshgen
+    from vbd_tetmesh_b200 import _capi, build_batch_solver, build_solver, meshgen
 
     meshes = meshgen.batched_blocks(args.batch_meshes)
     load = [0] * world
@@ -364,8 +364,11 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
         ms_b = timed(lambda: bs.step(dt, iters, g, True, rho))
         launches_b = (bs.kernel_launches() - l0) // (K + 1)
         xb = bs.get_positions()
+        batch_lanes = bs.get_option(_capi.OPT_LANES)
         bs.close()
-        plain = [build_solver(m, device=local, stream=stream.cuda_stream) for m in sub]
+        # the per-mesh solvers use the batch solver's lane count, so each mesh's arithmetic (and
+        # result) is the batch's
+        plain = [build_solver(m, device=local, stream=stream.cuda_stream, lanes=batch_lanes) for m in sub]
         l0 = sum(p.kernel_launches() for p in plain)
 
         def plain_step():
