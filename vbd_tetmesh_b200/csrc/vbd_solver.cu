@@ -220,9 +220,11 @@ struct vbd_solver {
                            keep_pp ? 1 : 0, cam.p};
         long long threads = (long long)(ve - vb) * lanes;
         vbd::SweepFn fn = vbd::pick_sweep(lanes, layout, prefetch != 0);
+        int threads_per_block = block;
         if (semantics) {
             threads = (long long)(ve - vb) * vbd::kWrapperLanes;
             fn = &vbd::k_sweep_wrapper;
+            threads_per_block = vbd::kWrapperBlock;
         }
         cudaEvent_t ev[2] = {nullptr, nullptr};
         if (timing) {
@@ -230,8 +232,8 @@ struct vbd_solver {
             CUDA_TRY(cudaEventRecord(ev[0], stream));
         }
         cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(vbd::nblk(threads, block));
-        cfg.blockDim = dim3(block);
+        cfg.gridDim = dim3(vbd::nblk(threads, threads_per_block));
+        cfg.blockDim = dim3(threads_per_block);
         cfg.dynamicSmemBytes = 0;
         cfg.stream = stream;
         cudaLaunchAttribute attr[1];
