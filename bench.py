@@ -326,16 +326,10 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
     import torch
 
     from vbd_tetmesh_b200 import _capi, build_batch_solver, build_solver, meshgen
+    from vbd_tetmesh_b200.sharding import combine_over_ranks, shard_meshes
 
     meshes = meshgen.batched_blocks(args.batch_meshes)
-    load = [0] * world
-    mine = []
-    for k in sorted(range(len(meshes)), key=lambda k: -meshes[k].num_tets):
-        r = min(range(world), key=lambda r: load[r])
-        load[r] += meshes[k].num_tets
-        if r == rank:
-            mine.append(k)
-    sub = [meshes[k] for k in sorted(mine)]
+    sub = [meshes[k] for k in shard_meshes([m.num_tets for m in meshes], world)[rank]]
     b = meshgen.concat(sub)
     dt, iters, rho, g = 1.0 / 60.0, 20, 0.9, (0.0, -9.8, 0.0)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
@@ -381,15 +375,8 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
         for p in plain:
             p.close()
     same = bool(np.array_equal(xb, xp))
-    t = torch.tensor([ms_b, ms_p, float(b.num_verts), 0.0 if same else 1.0], dtype=torch.float64,
-                     device=f"cuda:{local}")
-    if dist is not None:
-        tmax = t[:2].clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = t[2:].clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        t = torch.cat([tmax, tsum])
-    ms_b, ms_p, nverts, mism = (float(v) for v in t)
+    (ms_b, ms_p), (nverts, mism) = combine_over_ranks([ms_b, ms_p], [float(b.num_verts), 0.0 if same else 1.0],
+                                                      dist, f"cuda:{local}")
     units = nverts * iters * K
     allm = meshgen.concat(meshes)
     return {
@@ -599,10 +586,10 @@ def main():
         clock_info = clocks.stop()
 
     sing, nonf = solver.status()
-    t_max = torch.tensor([ms_total, e2e_s if not args.no_e2e else 0.0], dtype=torch.float64, device=f"cuda:{local}")
-    if dist is not None:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    ms_max, e2e_max = float(t_max[0]), float(t_max[1])
+    from vbd_tetmesh_b200.sharding import combine_over_ranks
+
+    (ms_max, e2e_max), _ = combine_over_ranks([ms_total, e2e_s if not args.no_e2e else 0.0], [], dist,
+                                              f"cuda:{local}")
     units = float(mesh.num_verts) * iters * args.steps * world
     value = units / (ms_max * 1e-3)
     if not args.no_e2e:
