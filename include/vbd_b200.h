@@ -239,7 +239,8 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
 /* Tuning knobs (all have measured defaults).
  *   VBD_OPT_LANES:       threads cooperating on one vertex: 1, 2, 4, 8, 16 or 32.  Until it is
  *                        set, vbd_solver_init picks 8 when the free vertices average at least 21
- *                        incident tets, else 4
+ *                        incident tets, else 4, then doubles it (up to 16) while the largest colour
+ *                        times the lanes stays within half of the GPU's resident threads
  *   VBD_OPT_LAYOUT:      0 = tet records gathered through a per-vertex tet list,
  *                        1 = 64 B tet records copied into incidence order and streamed,
  *                        2 = compact 56 B incidence records streamed (other three vertex ids, their
@@ -272,7 +273,10 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *                        tet records read through the per-vertex tet list (any layout), and
  *                        vbd_solver_step starting each sub-step from x = y as main.cpp's GPU loop
  *                        does.  Not with VBD_OPT_PERSISTENT, vbd_solver_record or the adjoint;
- *                        energies and residuals stay the Neo-Hookean ones */
+ *                        energies and residuals stay the Neo-Hookean ones
+ *   VBD_OPT_L2_PREFETCH: 1 = with the compact or factored layout, each colour sweep prefetches the
+ *                        records of the colour swept next into L2 (one bulk prefetch per block);
+ *                        off by default (slower on the measured meshes) */
 typedef enum vbd_option {
     VBD_OPT_LANES = 0,
     VBD_OPT_LAYOUT = 1,
@@ -283,7 +287,8 @@ typedef enum vbd_option {
     VBD_OPT_BLOCK = 6,
     VBD_OPT_PERSISTENT = 7,
     VBD_OPT_ADJOINT_ALTERNATE = 8,
-    VBD_OPT_SEMANTICS = 9
+    VBD_OPT_SEMANTICS = 9,
+    VBD_OPT_L2_PREFETCH = 10
 } vbd_option;
 int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value);
 int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value);

@@ -27,8 +27,9 @@ def test_batch_bit_identical_to_per_mesh_solvers(gpu_device, layout):
         s.step(1 / 60, 20, (0.0, -9.8, 0.0), True, 0.9)
     xb = b.split(s.get_positions())
     vb = b.split(s.get_velocities())
+    lanes = s.get_option(_capi.OPT_LANES)  # the per-mesh solvers run the batch's launch shape
     for m, x, v in zip(meshes, xb, vb):
-        p = build_solver(m, layout=layout)
+        p = build_solver(m, layout=layout, lanes=lanes)
         for _ in range(5):
             p.step(1 / 60, 20, (0.0, -9.8, 0.0), True, 0.9)
         np.testing.assert_array_equal(x, p.get_positions())

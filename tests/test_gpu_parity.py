@@ -149,3 +149,17 @@ def test_initial_velocity_and_stiff_material(gpu_device, seed):
     assert rel_err(g["x"], o["x"], m) < POS_TOL
     assert abs(g["ip"] - ip64) <= STIFF_IP_TOL_F64 * abs(ip64)
     assert abs(ip32 - ip64) <= STIFF_IP_TOL_F64 * abs(ip64)
+
+
+def test_l2_prefetch_option_changes_no_result(gpu_device):
+    """VBD_OPT_L2_PREFETCH only warms L2 with the next colour's records: bit-identical results."""
+    m = meshgen.cube(12)
+    s = meshgen.CUBE_SETTINGS
+    out = []
+    for pf in (0, 1):
+        for layout in (2, 3):
+            g = gpu_simulate(m, 2, s["dt"], s["iterations"], s["gravity"], True, s["rho"], layout=layout,
+                             options={_capi.OPT_L2_PREFETCH: pf})
+            out.append(g["x"])
+    np.testing.assert_array_equal(out[0], out[2])
+    np.testing.assert_array_equal(out[1], out[3])

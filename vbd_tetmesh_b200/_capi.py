@@ -38,6 +38,7 @@ OPT_BLOCK = 6
 OPT_PERSISTENT = 7
 OPT_ADJOINT_ALTERNATE = 8
 OPT_SEMANTICS = 9
+OPT_L2_PREFETCH = 10
 SEMANTICS_VBDSOLVER = 0
 SEMANTICS_GPU_WRAPPER = 1
 

@@ -49,6 +49,8 @@ struct SweepParams {
     int accel;                 // write x^(k) = omega (x~ - pp) + pp to xnext (VBD.cpp:290-300)
     int keep_pp;               // store the pre-sweep position into pp (VBD.cpp:78,89)
     const float* cam;          // V0 mu |q_n|^2 per incidence (layout 3; crec then holds factored records)
+    const char* l2_next;       // element records of the colour swept next (16 B aligned), prefetched
+    unsigned long long l2_bytes;  // into L2 while this colour runs; 0 = none
 };
 
 // Programmatic dependent launch: let the next kernel in the stream start its prologue now, and
@@ -465,6 +467,25 @@ __device__ __forceinline__ void vertex_update(const SweepParams& p, int v, int l
     if (p.keep_pp) p.pp[v] = xi;
 }
 
+// This block's share of [base, base + bytes) prefetched into L2 with one bulk prefetch
+// (cp.async.bulk.prefetch: no shared memory, no completion to wait for).  The share is a
+// 16-byte-aligned slice that stays inside the range; bytes is a multiple of 16 and base is
+// 16-byte aligned.
+__device__ __forceinline__ void l2_prefetch_share(const char* base, unsigned long long bytes) {
+    const unsigned long long units = bytes >> 4;
+    const unsigned long long per = (units + gridDim.x - 1) / gridDim.x;
+    const unsigned long long first = per * blockIdx.x;
+    if (first >= units) return;
+    unsigned long long n = units - first < per ? units - first : per;
+    const char* ptr = base + (first << 4);
+    while (n) {
+        const unsigned chunk = n > (1ull << 20) ? (1u << 20) : (unsigned)n;  // 16 MiB per instruction
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(ptr), "r"(chunk << 4) : "memory");
+        ptr += (unsigned long long)chunk << 4;
+        n -= chunk;
+    }
+}
+
 // One colour of one Gauss-Seidel sweep per launch (VBDsolver::solve, VBD.cpp:114-158).  Element
 // data never changes during a sweep, so the lane's first record is fetched before the dependency
 // wait; positions are read only after it.
@@ -482,6 +503,7 @@ __global__ void __launch_bounds__(256) k_sweep(SweepParams p) {
     const int j = j0 + lane;
     typename Elem<LAYOUT>::Rec nxt;
     if (PREFETCH && j < j1) nxt = Elem<LAYOUT>::fetch(p, j);
+    if (p.l2_bytes && threadIdx.x == 0) l2_prefetch_share(p.l2_next, p.l2_bytes);
     pdl_trigger();
     pdl_wait();
     vertex_update<LANES, LAYOUT, PREFETCH, false>(p, v, lane, active, j, j1, nxt);
@@ -594,7 +616,30 @@ constexpr int kWrapperLanes = 16;
 // of 20.4 ms for a 50-iteration solve on the 64^3 cube.
 constexpr int kWrapperBlock = 256;
 
-__global__ void __launch_bounds__(kWrapperBlock) k_sweep_wrapper(SweepParams p) {
+// Its parameter block is its own (the fields it reads, in SweepParams's order): the kernel's
+// compiled arithmetic was checked bit for bit with this block, and a different block layout has
+// been seen to change nvcc's fused multiply-add choices in it.
+struct WrapperParams {
+    float4* x;
+    float4* xnext;
+    float4* pp;
+    const float4* y;
+    const int* inc_off;
+    const int* inc_tet;
+    const TetRec* rec;
+    const TetRec* irec;
+    const int4* crec;
+    const float2* cmat;
+    unsigned long long* status;
+    int v_begin, v_end;
+    float dtsr;
+    float omega;
+    int accel;
+    int keep_pp;
+    const float* cam;
+};
+
+__global__ void __launch_bounds__(kWrapperBlock) k_sweep_wrapper(WrapperParams p) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & (kWrapperLanes - 1);
     const int v = p.v_begin + t / kWrapperLanes;
@@ -614,7 +659,7 @@ __global__ void __launch_bounds__(kWrapperBlock) k_sweep_wrapper(SweepParams p) 
 #pragma unroll
     for (int k = 0; k < 3; ++k) fs[k] = 0.0f;
     for (; j < j1; j += kWrapperLanes) {
-        const TetRec r = Elem<0>::fetch(p, j);
+        const TetRec r = load_rec(p.rec + __ldg(p.inc_tet + j));
         float H[9], g[3];
         if (corot_block(r, v, xi, p.x, H, g)) {
 #pragma unroll

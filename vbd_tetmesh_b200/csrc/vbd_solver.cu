@@ -90,7 +90,7 @@ static SweepFn pick_sweep(int lanes, int layout, bool prefetch) {
 // Key of a captured step / solve graph: everything baked into its kernel parameters.
 struct GraphKey {
     int kind;  // 0 = step, 1 = solve, 2 = single sweep
-    int iters, accel, init, lanes, layout, prefetch, pdl, block, semantics;
+    int iters, accel, init, lanes, layout, prefetch, pdl, block, semantics, l2_prefetch, src;
     float h, dtsr, hg[3], rho;
     bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
 };
@@ -125,10 +125,19 @@ struct vbd_solver {
     // defaults: the fastest shape measured on the 64^3 cube (compact streamed records, 4 lanes per
     // vertex, record prefetch, programmatic dependent launch, 128-thread blocks)
     int lanes = 8, layout = 3, use_graph = 1, timing = 0, prefetch = 1, pdl = 1, block = 64;
-    // Until VBD_OPT_LANES is set, init picks the lane count from the mean number of incident tets
-    // per free vertex: 8 lanes from 21 up (the 64^3 cube: 22.9, 5.09 vs 5.49 ms/step with 4), else 4
-    // (the 512-block batch: 19.5, 9.06 vs 10.2 ms/step with 8).
+    // Until VBD_OPT_LANES is set, init picks the lane count: 8 lanes when the free vertices average
+    // at least 21 incident tets (the 64^3 cube: 22.9, 5.04 vs 5.49 ms/step with 4), else 4 (the
+    // 512-block batch: 19.5, 9.06 vs 10.2 ms/step with 8); then doubled, up to 16, while the
+    // largest colour would still fill less than half of the GPU's resident threads (1024 per SM at
+    // this kernel's 64 registers): a small mesh leaves SMs idle, and more lanes per vertex shorten
+    // each vertex's dependent chain (the 2,673-vertex beam: 24.7 / 19.3 / 17.2 ms per 30 steps
+    // with 4 / 8 / 16 lanes).
     bool lanes_auto = true;
+    // VBD_OPT_L2_PREFETCH: each colour sweep prefetches the next colour's streamed records into L2.
+    // Off by default: on the 64^3 cube it measured 5.48 against 4.78 ms/step (the extra DRAM
+    // traffic competes with the running colour's own stream).
+    int l2_prefetch = 0;
+    std::vector<long long> colour_inc;  // first incidence of each colour (C + 1 entries)
     // VBD_OPT_SEMANTICS: 0 = VBDsolver (VBD.cpp), 1 = VBD_GPU_Solver (VBD_GPU_Wrapper.cu)
     int semantics = 0;
     float omega_next(int k, float rho, float prev) const {
@@ -150,6 +159,9 @@ struct vbd_solver {
     int ckpt_every = 0;
     std::vector<std::unique_ptr<vbd::DBuf<float4>>> ckpts;  // 2N each: x then v
     vbd::DBuf<float4> adj_lam, adj_lam2, adj_lpp, adj_G, adj_ax, adj_av, adj_seg, adj_save;
+    // converged positions of the recorded sub-steps of the newest segment, kept as the forward runs
+    // so that the backward starts without recomputing that segment
+    vbd::DBuf<float4> live_seg;
     vbd::DBuf<float> adj_gmu, adj_glam;
     int adj_cur = 0;  // which of adj_lam / adj_lam2 holds lam
     long long launches = 0;
@@ -218,14 +230,17 @@ struct vbd_solver {
         vbd::SweepParams p{xr,     xn,     pp.p,     y.p, inc_off.p, inc_tet.p, rec.p,          irec.p,
                            crec.p, cmat.p, status.p, vb,  ve,        dtsr,      omega, accel ? 1 : 0,
                            keep_pp ? 1 : 0, cam.p};
+        if (l2_prefetch && (layout == 2 || layout == 3) && crec.p && C > 0) {
+            // the colour swept after this one (colour 0 of the next iteration after the last)
+            const int cn = (c + 1) % C;
+            const long long j0 = colour_inc[cn], j1 = colour_inc[cn + 1];
+            p.l2_next = reinterpret_cast<const char*>(crec.p + 3 * j0);
+            p.l2_bytes = (unsigned long long)(j1 - j0) * 48ull;
+        }
         long long threads = (long long)(ve - vb) * lanes;
         vbd::SweepFn fn = vbd::pick_sweep(lanes, layout, prefetch != 0);
         int threads_per_block = block;
-        if (semantics) {
-            threads = (long long)(ve - vb) * vbd::kWrapperLanes;
-            fn = &vbd::k_sweep_wrapper;
-            threads_per_block = vbd::kWrapperBlock;
-        }
+        if (semantics) threads = (long long)(ve - vb) * vbd::kWrapperLanes;
         cudaEvent_t ev[2] = {nullptr, nullptr};
         if (timing) {
             VBD_TRY(timing_event(ev));
@@ -241,7 +256,15 @@ struct vbd_solver {
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
         cfg.numAttrs = (pdl && !timing) ? 1 : 0;
-        CUDA_TRY(cudaLaunchKernelEx(&cfg, fn, p));
+        if (semantics) {
+            const vbd::WrapperParams w{p.x,    p.xnext,  p.pp,    p.y,    p.inc_off, p.inc_tet, p.rec,   p.irec,  p.crec,
+                                       p.cmat, p.status, p.v_begin, p.v_end, p.dtsr, p.omega, p.accel, p.keep_pp, p.cam};
+            cfg.gridDim = dim3(vbd::nblk(threads, vbd::kWrapperBlock));
+            cfg.blockDim = dim3(vbd::kWrapperBlock);
+            CUDA_TRY(cudaLaunchKernelEx(&cfg, &vbd::k_sweep_wrapper, w));
+        } else {
+            CUDA_TRY(cudaLaunchKernelEx(&cfg, fn, p));
+        }
         VBD_TRY(check_launch());
         if (timing) {
             CUDA_TRY(cudaEventRecord(ev[1], stream));
@@ -392,6 +415,9 @@ struct vbd_solver {
         if (!ckpt_every) return VBD_OK;
         TapeStep t{h, dtsr, {hg[0], hg[1], hg[2]}, rho, iters, accel ? 1 : 0};
         tape.push_back(t);
+        const size_t slot = (tape.size() - 1) % (size_t)ckpt_every;
+        CUDA_TRY(cudaMemcpyAsync(live_seg.p + slot * (size_t)N, x0.p, sizeof(float4) * (size_t)N,
+                                 cudaMemcpyDeviceToDevice, stream));
         if (tape.size() % (size_t)ckpt_every == 0) {
             ckpts.emplace_back(new vbd::DBuf<float4>());
             VBD_TRY(ckpts.back()->alloc(2 * (size_t)N));
@@ -412,6 +438,7 @@ struct vbd_solver {
         key.pdl = pdl;
         key.block = block;
         key.semantics = semantics;
+        key.l2_prefetch = l2_prefetch;
         key.h = t.h;
         key.dtsr = t.dtsr;
         key.hg[0] = t.hg[0];
@@ -504,9 +531,12 @@ struct vbd_solver {
 
     // The adjoint sequence of a sub-step is replayed as a graph keyed by its parameters, the
     // positions slot it reads and which adjoint buffer is live.
-    int adjoint_substep(const TapeStep& t, int slot, const float4* X, int sweeps, float rho) {
+    // `src` tells the state buffers apart (0 = recomputed segment, 1 = kept newest segment): the
+    // captured graph bakes X's address.
+    int adjoint_substep(const TapeStep& t, int slot, const float4* X, int sweeps, float rho, int src) {
         vbd::GraphKey key{};
         key.kind = 3 + slot;
+        key.src = src;
         key.iters = sweeps;
         key.init = adj_cur;
         key.lanes = lanes;
@@ -838,7 +868,17 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     CUDA_TRY(cudaMemcpy(s->rec.p, rec.data(), sizeof(vbd::TetRec) * rec.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemset(s->status.p, 0, sizeof(unsigned long long) * vbd::ST_SLOTS));
 
-    if (s->lanes_auto) s->lanes = (nfree > 0 && (double)ninc >= 21.0 * nfree) ? 8 : 4;
+    if (s->lanes_auto) {
+        int L = (nfree > 0 && (double)ninc >= 21.0 * nfree) ? 8 : 4;
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+        long long largest = 0;
+        for (int c = 0; c < num_colours; ++c) largest = std::max<long long>(largest, cstart[c + 1] - cstart[c]);
+        while (L < 16 && largest * L * 2 <= (long long)sms * 1024) L *= 2;
+        s->lanes = L;
+    }
+    s->colour_inc.assign(num_colours + 1, 0);
+    for (int c = 0; c <= num_colours; ++c) s->colour_inc[c] = inc_off[cstart[c]];
     s->colour_bytes.assign(num_colours, 0.0);
     for (int c = 0; c < num_colours; ++c)
         for (int i = cstart[c]; i < cstart[c + 1]; ++i)
@@ -1009,6 +1049,7 @@ int vbd_solver_solve(vbd_solver* s, int32_t iterations, float dt_sqr_reciprocal,
     key.pdl = s->pdl;
     key.block = s->block;
     key.semantics = s->semantics;
+    key.l2_prefetch = s->l2_prefetch;
     key.dtsr = dt_sqr_reciprocal;
     key.rho = rho;
     if (s->persistent && !s->timing)
@@ -1052,6 +1093,7 @@ int vbd_solver_step(vbd_solver* s, float dt, int32_t substeps, int32_t iteration
     key.pdl = s->pdl;
     key.block = s->block;
     key.semantics = s->semantics;
+    key.l2_prefetch = s->l2_prefetch;
     key.h = h;
     key.dtsr = dtsr;
     key.hg[0] = hg[0];
@@ -1079,6 +1121,10 @@ int vbd_solver_record(vbd_solver* s, int32_t checkpoint_every) {
     s->ckpts.clear();
     s->ckpt_every = checkpoint_every;
     if (checkpoint_every > 0) {
+        if (s->live_seg.n != (size_t)checkpoint_every * s->N) {
+            s->drop_graphs();
+            VBD_TRY(s->live_seg.alloc((size_t)checkpoint_every * s->N));
+        }
         s->ckpts.emplace_back(new vbd::DBuf<float4>());
         VBD_TRY(s->ckpts.back()->alloc(2 * (size_t)s->N));
         VBD_TRY(s->snapshot(*s->ckpts.back()));
@@ -1134,19 +1180,25 @@ int vbd_solver_backward(vbd_solver* s, const float* dl_dx, const float* dl_dv, i
     int rc = VBD_OK;
     for (int seg = nseg - 1; seg >= 0 && !rc; --seg) {
         const int t0 = seg * K, t1 = std::min(nsteps, t0 + K);
-        vbd::DBuf<float4>& ck = *s->ckpts[seg];
-        CUDA_TRY(cudaMemcpyAsync(s->x0.p, ck.p, b4, cudaMemcpyDeviceToDevice, s->stream));
-        CUDA_TRY(cudaMemcpyAsync(s->x1.p, ck.p, b4, cudaMemcpyDeviceToDevice, s->stream));
-        CUDA_TRY(cudaMemcpyAsync(s->v.p, ck.p + N, b4, cudaMemcpyDeviceToDevice, s->stream));
-        for (int t = t0; t < t1 && !rc; ++t) {
-            rc = s->replay_substep(s->tape[t]);
-            if (!rc && cudaMemcpyAsync(s->adj_seg.p + (size_t)(t - t0) * N, s->x0.p, b4, cudaMemcpyDeviceToDevice,
-                                       s->stream) != cudaSuccess)
-                VBD_FAIL(VBD_ERR_CUDA, "segment copy failed");
+        // the newest segment's converged states were kept during the forward; older segments are
+        // recomputed from their checkpoint (same graphs, hence the same bits)
+        const bool live = seg == nseg - 1;
+        float4* states = live ? s->live_seg.p : s->adj_seg.p;
+        if (!live) {
+            vbd::DBuf<float4>& ck = *s->ckpts[seg];
+            CUDA_TRY(cudaMemcpyAsync(s->x0.p, ck.p, b4, cudaMemcpyDeviceToDevice, s->stream));
+            CUDA_TRY(cudaMemcpyAsync(s->x1.p, ck.p, b4, cudaMemcpyDeviceToDevice, s->stream));
+            CUDA_TRY(cudaMemcpyAsync(s->v.p, ck.p + N, b4, cudaMemcpyDeviceToDevice, s->stream));
+            for (int t = t0; t < t1 && !rc; ++t) {
+                rc = s->replay_substep(s->tape[t]);
+                if (!rc && cudaMemcpyAsync(s->adj_seg.p + (size_t)(t - t0) * N, s->x0.p, b4,
+                                           cudaMemcpyDeviceToDevice, s->stream) != cudaSuccess)
+                    VBD_FAIL(VBD_ERR_CUDA, "segment copy failed");
+            }
         }
         for (int t = t1 - 1; t >= t0 && !rc; --t)
-            rc = s->adjoint_substep(s->tape[t], t - t0, s->adj_seg.p + (size_t)(t - t0) * N, adjoint_iterations,
-                                    adjoint_rho);
+            rc = s->adjoint_substep(s->tape[t], t - t0, states + (size_t)(t - t0) * N, adjoint_iterations,
+                                    adjoint_rho, live ? 1 : 0);
     }
     if (!rc) {
         if (dl_dx0) rc = s->download3(s->adj_ax.p, dl_dx0);
@@ -1276,6 +1328,9 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
                 VBD_FAIL(VBD_ERR_INVALID_ARG, "the persistent kernel runs the VBDsolver semantics only");
             s->persistent = value ? 1 : 0;
             return VBD_OK;
+        case VBD_OPT_L2_PREFETCH:
+            s->l2_prefetch = value ? 1 : 0;
+            return VBD_OK;
         case VBD_OPT_SEMANTICS:
             if (value != 0 && value != 1) VBD_FAIL(VBD_ERR_INVALID_ARG, "semantics must be 0 (VBDsolver) or 1 (VBD_GPU_Solver)");
             if (value && s->persistent)
@@ -1324,6 +1379,7 @@ int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value) {
         case VBD_OPT_BLOCK: *value = s->block; return VBD_OK;
         case VBD_OPT_PERSISTENT: *value = s->persistent; return VBD_OK;
         case VBD_OPT_SEMANTICS: *value = s->semantics; return VBD_OK;
+        case VBD_OPT_L2_PREFETCH: *value = s->l2_prefetch; return VBD_OK;
         case VBD_OPT_ADJOINT_ALTERNATE: *value = s->adj_alternate; return VBD_OK;
         default: VBD_FAIL(VBD_ERR_INVALID_ARG, "unknown option %d", option);
     }
