@@ -612,8 +612,10 @@ constexpr int kWrapperLanes = 16;
 
 // Tet records are read through the per-vertex tet list whatever the layout option, as the
 // reference's kernel reads them; this one code path is the one checked bit for bit against it.
-// Records are loaded where they are used (no prefetch): 79 instead of 99 registers, 16.5 instead
-// of 20.4 ms for a 50-iteration solve on the 64^3 cube.
+// Records are loaded where they are used (no prefetch) and the kernel is held to 64 registers (4
+// blocks of 256 per SM, a few bytes of spill): 15.2 ms for a 50-iteration solve on the 64^3 cube,
+// against 20.4 ms with prefetch at 99 registers and 16.5 ms at 79.  Tighter caps spill heavily,
+// run slower, and change ptxas's fused multiply-add choices (no longer bit-identical).
 constexpr int kWrapperBlock = 256;
 
 // Its parameter block is its own (the fields it reads, in SweepParams's order): the kernel's
@@ -639,7 +641,7 @@ struct WrapperParams {
     const float* cam;
 };
 
-__global__ void __launch_bounds__(kWrapperBlock) k_sweep_wrapper(WrapperParams p) {
+__global__ void __launch_bounds__(kWrapperBlock, 4) k_sweep_wrapper(WrapperParams p) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & (kWrapperLanes - 1);
     const int v = p.v_begin + t / kWrapperLanes;
