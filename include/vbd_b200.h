@@ -245,7 +245,7 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *                        1 = 64 B tet records copied into incidence order and streamed,
  *                        2 = compact 56 B incidence records streamed (other three vertex ids, their
  *                            rows of Ps Dm^-1, V0 mu, V0 lambda)
- *                        3 = factored 52 B incidence records streamed (other three vertex ids,
+ *                        3 = factored 48 B incidence records streamed (other three vertex ids,
  *                            s = M q_n, w = cof(M) q_n, det M for M = their rows of Ps Dm^-1, and the
  *                            material products): the element block without forming F or cof(F);
  *                            the default

@@ -48,7 +48,10 @@ struct SweepParams {
     float omega;
     int accel;                 // write x^(k) = omega (x~ - pp) + pp to xnext (VBD.cpp:290-300)
     int keep_pp;               // store the pre-sweep position into pp (VBD.cpp:78,89)
-    const float* cam;          // V0 mu |q_n|^2 per incidence (layout 3; crec then holds factored records)
+    // Unused by the kernels.  It keeps this block at 136 bytes: on the 64^3 cube the step measured
+    // 4.61 ms with 136 bytes, 4.81 ms with 128 and 5.05 ms with 120 (A/B on one B200, kernel
+    // arithmetic unchanged); the cause is not known.
+    const void* reserved;
     const char* l2_next;       // element records of the colour swept next (16 B aligned), prefetched
     unsigned long long l2_bytes;  // into L2 while this colour runs; 0 = none
 };
@@ -272,7 +275,7 @@ __device__ __forceinline__ void compact_contrib(const CompactRec& r, float4 xi, 
     }
 }
 
-// Factored incidence record (layout 3), 48 B + 4 B per (vertex, tet) incidence.  With M the 3x3
+// Factored incidence record (layout 3), 48 B per (vertex, tet) incidence.  With M the 3x3
 // matrix whose rows are q_k of the three other vertices (the compact record's q) and q_n their
 // negated sum, F = D M for D = [d_0 d_1 d_2], d_k = x_k - x_n.  Hence
 //   F q_n = D s,          s = M q_n
@@ -284,13 +287,14 @@ __device__ __forceinline__ void compact_contrib(const CompactRec& r, float4 xi, 
 //   int4  {nb0 | n << 30, nb1, nb2, s0}
 //   float4{s1, s2, w0, w1}
 //   float4{w2, det M, V0 mu, V0 lambda}
-//   float  V0 mu |q_n|^2                        (separate stream)
+// |q_n|^2 (for the Hessian's V0 mu |q_n|^2 I term) is -(s0 + s1 + s2), since the rows of Q sum to
+// zero; it is not stored (a 4 B stream per incidence cost 0.17 ms of the cube's 4.78 ms step).
 struct FactRec {
     int nb0, nb1, nb2;
     float s0, s1, s2, w0, w1, w2, detm, a, b, am;
 };
 
-__device__ __forceinline__ FactRec load_fact(const int4* __restrict__ crec, const float* __restrict__ cam, int j) {
+__device__ __forceinline__ FactRec load_fact(const int4* __restrict__ crec, int j) {
     const int4 w0 = __ldg(crec + 3 * j);
     const float4 w1 = __ldg(reinterpret_cast<const float4*>(crec) + 3 * j + 1);
     const float4 w2 = __ldg(reinterpret_cast<const float4*>(crec) + 3 * j + 2);
@@ -307,7 +311,10 @@ __device__ __forceinline__ FactRec load_fact(const int4* __restrict__ crec, cons
     r.detm = w2.y;
     r.a = w2.z;
     r.b = w2.w;
-    r.am = __ldg(cam + j);
+    // V0 mu |q_n|^2: the rows of Q sum to zero, so sum_k s_k = sum_k q_k . q_n = -|q_n|^2.  Rounded
+    // on its own (no fused multiply-add into the Hessian sums), so every launch shape computes it
+    // identically.
+    r.am = __fmul_rn(r.a, -(r.s0 + r.s1 + r.s2));
     return r;
 }
 
@@ -393,7 +400,7 @@ template <> struct Elem<2> {
 };
 template <> struct Elem<3> {
     using Rec = FactRec;
-    __device__ __forceinline__ static Rec fetch(const SweepParams& p, int j) { return load_fact(p.crec, p.cam, j); }
+    __device__ __forceinline__ static Rec fetch(const SweepParams& p, int j) { return load_fact(p.crec, j); }
     template <bool COHERENT>
     __device__ __forceinline__ static void contrib(const Rec& r, int, float4 xi, const float4* X, Acc& acc) {
         fact_contrib<true, COHERENT>(r, xi, X, acc);
@@ -1029,7 +1036,7 @@ __global__ void k_pack_compact(const TetRec* __restrict__ rec, const int* __rest
 // Factored records (layout 3) from the tet records: M's rows in the compact record's order, then
 // s = M q_n, w = cof(M) q_n, det M and the material products.
 __global__ void k_pack_factored(const TetRec* __restrict__ rec, const int* __restrict__ inc_tet,
-                                const int* __restrict__ inc_vertex, int4* __restrict__ crec, float* __restrict__ cam,
+                                const int* __restrict__ inc_vertex, int4* __restrict__ crec,
                                 int ninc) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ninc) return;
@@ -1078,7 +1085,6 @@ __global__ void k_pack_factored(const TetRec* __restrict__ rec, const int* __res
     crec[3 * j] = make_int4(nb[0] | (n << 30), nb[1], nb[2], __float_as_int(sv[0]));
     crec[3 * j + 1] = make_int4(__float_as_int(sv[1]), __float_as_int(sv[2]), __float_as_int(wv[0]), __float_as_int(wv[1]));
     crec[3 * j + 2] = make_int4(__float_as_int(wv[2]), __float_as_int(detm), __float_as_int(a), __float_as_int(b));
-    cam[j] = a * (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
 }
 
 // ---- implicit adjoint of a converged step --------------------------------------------------
@@ -1241,7 +1247,6 @@ struct AdjParams {
     float omega;
     int accel;                // write lam_next
     int keep_pp;              // store the pre-sweep adjoint into lam_pp
-    const float* cam;         // factored records' V0 mu |q_n|^2 (layout 3; crec holds factored records)
 };
 
 template <int LAYOUT> struct AdjElem;
@@ -1255,7 +1260,7 @@ template <> struct AdjElem<2> {
 };
 template <> struct AdjElem<3> {
     using Rec = FactRec;
-    __device__ __forceinline__ static Rec fetch(const AdjParams& p, int j) { return load_fact(p.crec, p.cam, j); }
+    __device__ __forceinline__ static Rec fetch(const AdjParams& p, int j) { return load_fact(p.crec, j); }
 };
 
 // Adjoint element terms from a factored record (F = D M, dF = L M with L = [lam_0 lam_1 lam_2]):

@@ -117,7 +117,6 @@ struct vbd_solver {
     vbd::DBuf<vbd::TetRec> rec, irec;
     vbd::DBuf<int4> crec;                           // compact (layout 2) or factored (layout 3) records
     vbd::DBuf<float2> cmat;
-    vbd::DBuf<float> cam;                           // factored layout: V0 mu |q_n|^2 per incidence
     vbd::DBuf<int> inc_vertex;                      // internal vertex of each incidence
     vbd::DBuf<float> stage, mat_stage;
     vbd::DBuf<unsigned long long> status;
@@ -229,7 +228,7 @@ struct vbd_solver {
         if (ve <= vb) return VBD_OK;
         vbd::SweepParams p{xr,     xn,     pp.p,     y.p, inc_off.p, inc_tet.p, rec.p,          irec.p,
                            crec.p, cmat.p, status.p, vb,  ve,        dtsr,      omega, accel ? 1 : 0,
-                           keep_pp ? 1 : 0, cam.p};
+                           keep_pp ? 1 : 0, nullptr};
         if (l2_prefetch && (layout == 2 || layout == 3) && crec.p && C > 0) {
             // the colour swept after this one (colour 0 of the next iteration after the last)
             const int cn = (c + 1) % C;
@@ -258,7 +257,7 @@ struct vbd_solver {
         cfg.numAttrs = (pdl && !timing) ? 1 : 0;
         if (semantics) {
             const vbd::WrapperParams w{p.x,    p.xnext,  p.pp,    p.y,    p.inc_off, p.inc_tet, p.rec,   p.irec,  p.crec,
-                                       p.cmat, p.status, p.v_begin, p.v_end, p.dtsr, p.omega, p.accel, p.keep_pp, p.cam};
+                                       p.cmat, p.status, p.v_begin, p.v_end, p.dtsr, p.omega, p.accel, p.keep_pp, nullptr};
             cfg.gridDim = dim3(vbd::nblk(threads, vbd::kWrapperBlock));
             cfg.blockDim = dim3(vbd::kWrapperBlock);
             CUDA_TRY(cudaLaunchKernelEx(&cfg, &vbd::k_sweep_wrapper, w));
@@ -377,7 +376,7 @@ struct vbd_solver {
         const int grid = per_sm * sms;
         vbd::PersistParams pp_{};
         pp_.sw = vbd::SweepParams{x0.p, x1.p, pp.p, y.p,  inc_off.p, inc_tet.p, rec.p, irec.p, crec.p, cmat.p,
-                                  status.p, 0,  0,    dtsr, 1.0f,      0,         accel ? 1 : 0, cam.p};
+                                  status.p, 0,  0,    dtsr, 1.0f,      0,         accel ? 1 : 0, nullptr};
         pp_.xa = x0.p;
         pp_.xb = x1.p;
         pp_.v = v.p;
@@ -472,7 +471,7 @@ struct vbd_solver {
             float4* lo = cur ? adj_lam.p : adj_lam2.p;
             vbd::AdjParams ap{X,         lr,      adj_G.p, y.p,   inc_off.p,     inc_tet.p,     rec.p,
                               crec.p,    cmat.p,  t.dtsr,  0,     0,             lo,            adj_lpp.p,
-                              omega,     blend ? 1 : 0,    accel ? 1 : 0, cam.p};
+                              omega,     blend ? 1 : 0,    accel ? 1 : 0};
             const int alay = (layout == 2 || layout == 3) ? layout : 0;
             for (int k = 0; k < C; ++k) {
                 const int col = (adj_alternate && (it % 2 == 0)) ? C - 1 - k : k;
@@ -516,7 +515,7 @@ struct vbd_solver {
         if (N > nfree) {
             vbd::AdjParams ap{X,      lam,     adj_G.p, y.p,  inc_off.p, inc_tet.p, rec.p,
                               crec.p, cmat.p,  t.dtsr,  nfree, N,        nullptr,   nullptr,
-                              1.0f,   0,       0, cam.p};
+                              1.0f,   0,       0};
             const unsigned grid = vbd::nblk((long long)(N - nfree) * 8, 256);
             vbd::k_adj_pinned<8><<<grid, 256, 0, stream>>>(ap, adj_ax.p);
             VBD_TRY(check_launch());
@@ -621,10 +620,6 @@ struct vbd_solver {
             drop_graphs();
             cmat.release();
         }
-        if (layout != 3 && cam.p) {
-            drop_graphs();
-            cam.release();
-        }
         if (layout != 2 && layout != 3 && crec.p) {
             drop_graphs();
             crec.release();
@@ -647,17 +642,13 @@ struct vbd_solver {
                 drop_graphs();
                 VBD_TRY(cmat.alloc(ninc));
             }
-            if (layout == 3 && cam.n != (size_t)ninc) {
-                drop_graphs();
-                VBD_TRY(cam.alloc(ninc));
-            }
             if (ninc > 0 && layout == 2) {
                 vbd::k_pack_compact<<<vbd::nblk(ninc, 256), 256, 0, stream>>>(rec.p, inc_tet.p, inc_vertex.p, crec.p,
                                                                              cmat.p, (int)ninc);
                 VBD_TRY(check_launch());
             } else if (ninc > 0) {
                 vbd::k_pack_factored<<<vbd::nblk(ninc, 256), 256, 0, stream>>>(rec.p, inc_tet.p, inc_vertex.p, crec.p,
-                                                                              cam.p, (int)ninc);
+                                                                              (int)ninc);
                 VBD_TRY(check_launch());
             }
         }
@@ -785,7 +776,6 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     s->irec.release();
     s->crec.release();
     s->cmat.release();
-    s->cam.release();
 
     // Internal order: free vertices colour by colour (group order), then the pinned ones.
     std::vector<int32_t> perm;
@@ -1266,7 +1256,7 @@ int vbd_solver_energy(vbd_solver* s, int32_t kind, float h, double* out) {
         }
         vbd::SweepParams p{s->x0.p,     nullptr, s->pp.p,    s->y.p, s->inc_off.p, s->inc_tet.p,
                            s->rec.p,    s->irec.p, s->crec.p, s->cmat.p, s->status.p, 0,
-                           s->nfree,    (float)(1.0 / ((double)h * h)), 1.0f, 0, 0, s->cam.p};
+                           s->nfree,    (float)(1.0 / ((double)h * h)), 1.0f, 0, 0, nullptr};
         const int L = std::max(4, s->lanes);
         const unsigned blocks = vbd::nblk((long long)s->nfree * L, 256);
         switch (L) {
