@@ -48,9 +48,9 @@ struct SweepParams {
     float omega;
     int accel;                 // write x^(k) = omega (x~ - pp) + pp to xnext (VBD.cpp:290-300)
     int keep_pp;               // store the pre-sweep position into pp (VBD.cpp:78,89)
-    // Unused by the kernels.  It keeps this block at 136 bytes: on the 64^3 cube the step measured
-    // 4.61 ms with 136 bytes, 4.81 ms with 128 and 5.05 ms with 120 (A/B on one B200, kernel
-    // arithmetic unchanged); the cause is not known.
+    // Unused by the kernels.  It keeps this block above 128 bytes: on the 64^3 cube the step
+    // measured 4.61 ms at 136 bytes (and the same at 152 to 264), 4.81 ms at 128 and 5.05 ms at
+    // 120 (A/B on one B200, kernel arithmetic unchanged); the cause is not known.
     const void* reserved;
     const char* l2_next;       // element records of the colour swept next (16 B aligned), prefetched
     unsigned long long l2_bytes;  // into L2 while this colour runs; 0 = none
