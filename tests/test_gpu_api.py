@@ -267,3 +267,20 @@ def test_layout_switches_rebuild_captured_graphs(gpu_device):
         s.step(1 / 60, 6, (0, -9.8, 0), True, 0.9)
     o = po.simulate(m, 5, 1 / 60, 6, (0, -9.8, 0), True, 0.9)
     assert rel_err(s.get_positions(), o["x"], m) < 1e-5
+
+
+def test_lane_count_chosen_at_init(gpu_device):
+    """Until VBD_OPT_LANES is set, init picks the lane count from the mesh: 8 for the 64^3 cube (mean
+    valence 22.9, colours large enough to fill the GPU), 16 for a small mesh that leaves SMs idle,
+    and an explicit setting sticks."""
+    from vbd_tetmesh_b200 import _capi
+
+    cube = build_solver(meshgen.cube(64))
+    assert cube.get_option(_capi.OPT_LANES) == 8
+    cube.close()
+    small = build_solver(meshgen.beam())
+    assert small.get_option(_capi.OPT_LANES) == 16
+    small.close()
+    fixed = build_solver(meshgen.beam(), lanes=4)
+    assert fixed.get_option(_capi.OPT_LANES) == 4
+    fixed.close()
