@@ -247,10 +247,14 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *                            rows of Ps Dm^-1, V0 mu, V0 lambda)
  *                        3 = factored 48 B incidence records streamed (other three vertex ids,
  *                            s = M q_n, w = cof(M) q_n, det M for M = their rows of Ps Dm^-1, and the
- *                            material products): the element block without forming F or cof(F);
- *                            the default
- *                        Defaults: layout 3, 64-thread blocks, prefetch, PDL, graphs; lanes
- *                        chosen by vbd_solver_init (below).
+ *                            material products): the element block without forming F or cof(F)
+ *                        4 = packed factored 40 B incidence records (the three ids in 21 bits
+ *                            each, s, w and the material products; det M = s.w / |q_n|^2 derived):
+ *                            meshes of at most 2^21 vertices only (VBD_ERR_INVALID_ARG otherwise)
+ *                        Until it is set, vbd_solver_init picks layout 4 when the mesh has at most
+ *                        2^21 vertices, else 3.
+ *                        Defaults: 64-thread blocks, prefetch, PDL, graphs; lanes and layout
+ *                        chosen by vbd_solver_init.
  *   VBD_OPT_GRAPH:       1 = replay a captured CUDA graph per step, 0 = direct launches
  *   VBD_OPT_KERNEL_TIMING: 1 = launch directly and bracket every colour-sweep kernel with a CUDA
  *                        event pair on the handle's stream (read with vbd_solver_kernel_time)

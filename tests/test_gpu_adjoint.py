@@ -89,7 +89,7 @@ def test_adjoint_matches_finite_differences(gpu_device):
         assert err < GRAD_RTOL
 
 
-@pytest.mark.parametrize("layout", [0, 2, 3])
+@pytest.mark.parametrize("layout", [0, 2, 3, 4])
 def test_adjoint_record_layouts_agree(gpu_device, layout):
     """The adjoint sweeps read the forward's record layout (gathered tet records, compact or
     factored incidence records); every layout must give the FP64 oracle's gradients."""

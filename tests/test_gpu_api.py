@@ -247,7 +247,7 @@ def test_autotune_restores_state_and_keeps_parity(gpu_device):
     x0 = s.get_positions()
     v0 = s.get_velocities()
     chosen = s.autotune(1 / 120, iterations=5, repeats=1)
-    assert chosen["lanes"] in (2, 4, 8, 16) and chosen["layout"] in (0, 1, 2, 3)
+    assert chosen["lanes"] in (2, 4, 8, 16) and chosen["layout"] in (0, 1, 2, 3, 4)
     np.testing.assert_array_equal(s.get_positions(), x0)
     np.testing.assert_array_equal(s.get_velocities(), v0)
     assert s.status() == (0, False)
@@ -262,10 +262,11 @@ def test_layout_switches_rebuild_captured_graphs(gpu_device):
     (same step parameters, so the same graph key) must use the new buffers."""
     m = small_block(seed=43)
     s = build_solver(m, layout=1)
-    for layout in (1, 0, 1, 0, 1):
+    seq = (1, 0, 4, 3, 4, 2, 1)
+    for layout in seq:
         s.set_option(_capi.OPT_LAYOUT, layout)
         s.step(1 / 60, 6, (0, -9.8, 0), True, 0.9)
-    o = po.simulate(m, 5, 1 / 60, 6, (0, -9.8, 0), True, 0.9)
+    o = po.simulate(m, len(seq), 1 / 60, 6, (0, -9.8, 0), True, 0.9)
     assert rel_err(s.get_positions(), o["x"], m) < 1e-5
 
 
@@ -284,3 +285,37 @@ def test_lane_count_chosen_at_init(gpu_device):
     fixed = build_solver(meshgen.beam(), lanes=4)
     assert fixed.get_option(_capi.OPT_LANES) == 4
     fixed.close()
+
+
+def _disjoint_tets(num_tets):
+    """num_tets separate unit-corner tets (4 vertices each), all placed at the origin."""
+    from vbd_tetmesh_b200.meshgen import Mesh
+
+    corner = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32) * 0.05
+    rest = np.tile(corner, (num_tets, 1))
+    tets = np.arange(4 * num_tets, dtype=np.int32).reshape(-1, 4)
+    mu, lam = meshgen.lame(1e5, 0.3)
+    return Mesh(rest=rest, x=rest.copy(), v=np.zeros_like(rest), tets=tets,
+                fixed=np.zeros(rest.shape[0], np.uint8), mu=np.full(num_tets, mu, np.float32),
+                lam=np.full(num_tets, lam, np.float32))
+
+
+def test_record_layout_chosen_at_init(gpu_device):
+    """Until VBD_OPT_LAYOUT is set, init picks the 40-byte packed factored records (layout 4) when
+    every vertex id fits their 21-bit fields, else the 48-byte factored records (layout 3); layout 4
+    is refused for a mesh with more than 2^21 vertices, at init and afterwards."""
+    small = build_solver(meshgen.cube(6))
+    assert small.get_option(_capi.OPT_LAYOUT) == 4
+    small.close()
+    big = _disjoint_tets((1 << 19) + 1)  # 2^21 + 4 vertices
+    s = build_solver(big)
+    assert s.get_option(_capi.OPT_LAYOUT) == 3
+    with pytest.raises(VBDError):
+        s.set_option(_capi.OPT_LAYOUT, 4)
+    assert s.get_option(_capi.OPT_LAYOUT) == 3
+    s.step(1 / 60, 3, (0.0, -9.8, 0.0), True, 0.9)
+    x = s.get_positions()
+    assert np.all(np.isfinite(x)) and s.status() == (0, False)
+    s.close()
+    with pytest.raises(VBDError):
+        build_solver(big, layout=4)

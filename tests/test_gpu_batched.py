@@ -15,7 +15,7 @@ def small_batch():
     return meshgen.batched_blocks(num_meshes=6, lo=2, hi=6, seed=7)
 
 
-@pytest.mark.parametrize("layout", [1, 2, 3])
+@pytest.mark.parametrize("layout", [1, 2, 3, 4])
 def test_batch_bit_identical_to_per_mesh_solvers(gpu_device, layout):
     meshes = small_batch()
     b = meshgen.concat(meshes)

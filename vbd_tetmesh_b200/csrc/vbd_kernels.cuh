@@ -40,8 +40,8 @@ struct SweepParams {
     const int* inc_tet;
     const TetRec* rec;
     const TetRec* irec;
-    const int4* crec;          // compact incidence records, 3 x int4 per incidence (layout 2)
-    const float2* cmat;        // (V0 mu, V0 lambda) per incidence (layout 2)
+    const int4* crec;          // streamed incidence records: 3 x int4 (layouts 2, 3) or 2 x int4 (layout 4)
+    const float2* cmat;        // (V0 mu, V0 lambda) per incidence (layouts 2, 4)
     unsigned long long* status;
     int v_begin, v_end;
     float dtsr;                // 1/h^2
@@ -294,27 +294,87 @@ struct FactRec {
     float s0, s1, s2, w0, w1, w2, detm, a, b, am;
 };
 
-__device__ __forceinline__ FactRec load_fact(const int4* __restrict__ crec, int j) {
-    const int4 w0 = __ldg(crec + 3 * j);
-    const float4 w1 = __ldg(reinterpret_cast<const float4*>(crec) + 3 * j + 1);
-    const float4 w2 = __ldg(reinterpret_cast<const float4*>(crec) + 3 * j + 2);
+// The raw words of a factored record.  A fetch only loads them; they are decoded where the record
+// is used, so no instruction waits on a prefetched record before the next prefetch is issued.
+struct FactRaw3 {
+    int4 w0;
+    float4 w1, w2;
+};
+
+__device__ __forceinline__ FactRaw3 load_fact(const int4* __restrict__ crec, int j) {
+    FactRaw3 r;
+    r.w0 = __ldg(crec + 3 * j);
+    r.w1 = __ldg(reinterpret_cast<const float4*>(crec) + 3 * j + 1);
+    r.w2 = __ldg(reinterpret_cast<const float4*>(crec) + 3 * j + 2);
+    return r;
+}
+
+__device__ __forceinline__ FactRec decode_fact(const FactRaw3& w) {
     FactRec r;
-    r.nb0 = w0.x & kCompactIdMask;
-    r.nb1 = w0.y;
-    r.nb2 = w0.z;
-    r.s0 = __int_as_float(w0.w);
-    r.s1 = w1.x;
-    r.s2 = w1.y;
-    r.w0 = w1.z;
-    r.w1 = w1.w;
-    r.w2 = w2.x;
-    r.detm = w2.y;
-    r.a = w2.z;
-    r.b = w2.w;
+    r.nb0 = w.w0.x & kCompactIdMask;
+    r.nb1 = w.w0.y;
+    r.nb2 = w.w0.z;
+    r.s0 = __int_as_float(w.w0.w);
+    r.s1 = w.w1.x;
+    r.s2 = w.w1.y;
+    r.w0 = w.w1.z;
+    r.w1 = w.w1.w;
+    r.w2 = w.w2.x;
+    r.detm = w.w2.y;
+    r.a = w.w2.z;
+    r.b = w.w2.w;
     // V0 mu |q_n|^2: the rows of Q sum to zero, so sum_k s_k = sum_k q_k . q_n = -|q_n|^2.  Rounded
     // on its own (no fused multiply-add into the Hessian sums), so every launch shape computes it
     // identically.
     r.am = __fmul_rn(r.a, -(r.s0 + r.s1 + r.s2));
+    return r;
+}
+
+// Packed factored record (layout 4), 40 B per incidence in two streams:
+//   int4  {ids.lo, ids.hi, s0, s1}    the other three vertices, 21 bits each in 64 bits
+//   float4{s2, w0, w1, w2}
+//   float2{V0 mu, V0 lambda}          (separate stream, as for layout 2)
+// det M is not stored: M^T cof(M) = det(M) I gives s . w = q_n^T M^T cof(M) q_n = det(M) |q_n|^2,
+// with |q_n|^2 = -(s0 + s1 + s2) as above.  The local index n is not needed by the factored form.
+// Ids must be below 2^21; the host keeps layout 3 for larger meshes.
+constexpr int kPackedIdBits = 21;
+constexpr int kPackedIdMask = (1 << kPackedIdBits) - 1;
+constexpr long long kPackedMaxVertices = 1LL << kPackedIdBits;
+
+struct FactRaw4 {
+    int4 w0;
+    float4 w1;
+    float2 m;
+};
+
+__device__ __forceinline__ FactRaw4 load_fact_packed(const int4* __restrict__ crec, const float2* __restrict__ cmat,
+                                                     int j) {
+    FactRaw4 r;
+    r.w0 = __ldg(crec + 2 * j);
+    r.w1 = __ldg(reinterpret_cast<const float4*>(crec) + 2 * j + 1);
+    r.m = __ldg(cmat + j);
+    return r;
+}
+
+__device__ __forceinline__ FactRec decode_fact(const FactRaw4& w) {
+    const unsigned lo = (unsigned)w.w0.x, hi = (unsigned)w.w0.y;
+    FactRec r;
+    r.nb0 = (int)(lo & kPackedIdMask);
+    r.nb1 = (int)(__funnelshift_r(lo, hi, kPackedIdBits) & kPackedIdMask);
+    r.nb2 = (int)((hi >> (2 * kPackedIdBits - 32)) & kPackedIdMask);
+    r.s0 = __int_as_float(w.w0.z);
+    r.s1 = __int_as_float(w.w0.w);
+    r.s2 = w.w1.x;
+    r.w0 = w.w1.y;
+    r.w1 = w.w1.z;
+    r.w2 = w.w1.w;
+    r.a = w.m.x;
+    r.b = w.m.y;
+    // Explicit roundings, so every launch shape derives the same det M and V0 mu |q_n|^2.
+    const float qq = -(r.s0 + r.s1 + r.s2);
+    const float sw = __fmaf_rn(r.s2, r.w2, __fmaf_rn(r.s1, r.w1, __fmul_rn(r.s0, r.w0)));
+    r.detm = __fdiv_rn(sw, qq);
+    r.am = __fmul_rn(r.a, qq);
     return r;
 }
 
@@ -370,7 +430,7 @@ __device__ __forceinline__ void group_reduce(Acc& a) {
 
 // Element data of incidence j under each record layout:
 //   0 = tet record gathered through inc_tet, 1 = tet record streamed in incidence order,
-//   2 = compact streamed record, 3 = factored streamed record.
+//   2 = compact streamed record, 3 = factored streamed record, 4 = packed factored record.
 template <int LAYOUT> struct Elem;
 template <> struct Elem<0> {
     using Rec = TetRec;
@@ -399,11 +459,22 @@ template <> struct Elem<2> {
     }
 };
 template <> struct Elem<3> {
-    using Rec = FactRec;
+    using Rec = FactRaw3;
     __device__ __forceinline__ static Rec fetch(const SweepParams& p, int j) { return load_fact(p.crec, j); }
     template <bool COHERENT>
     __device__ __forceinline__ static void contrib(const Rec& r, int, float4 xi, const float4* X, Acc& acc) {
-        fact_contrib<true, COHERENT>(r, xi, X, acc);
+        fact_contrib<true, COHERENT>(decode_fact(r), xi, X, acc);
+    }
+};
+
+template <> struct Elem<4> {
+    using Rec = FactRaw4;
+    __device__ __forceinline__ static Rec fetch(const SweepParams& p, int j) {
+        return load_fact_packed(p.crec, p.cmat, j);
+    }
+    template <bool COHERENT>
+    __device__ __forceinline__ static void contrib(const Rec& r, int, float4 xi, const float4* X, Acc& acc) {
+        fact_contrib<true, COHERENT>(decode_fact(r), xi, X, acc);
     }
 };
 
@@ -413,7 +484,7 @@ template <> struct Elem<3> {
 // |det| > 1e-8 guard (VBD.cpp:141-152, Types.h:85-112), then writes x~, the Chebyshev blend
 // x^(k) = omega (x~ - pp) + pp (VBD.cpp:290-300) and the pre-sweep position into pp.
 // Every lane of the warp must call it (shuffles); `active` marks lanes with a real vertex.
-//   LAYOUT   : element record layout (Elem<0/1/2>)
+//   LAYOUT   : element record layout (Elem<0..4>)
 //   PREFETCH : the next element record is loaded while the current one is evaluated
 //   COHERENT : positions read with coherent loads (persistent kernel)
 // `nxt` holds the lane's first record if PREFETCH (fetched by the caller).
@@ -1033,11 +1104,13 @@ __global__ void k_pack_compact(const TetRec* __restrict__ rec, const int* __rest
     cmat[j] = make_float2(r.c.y * r.c.z, r.c.y * r.c.w);
 }
 
-// Factored records (layout 3) from the tet records: M's rows in the compact record's order, then
-// s = M q_n, w = cof(M) q_n, det M and the material products.
+// Factored records from the tet records: M's rows in the compact record's order, then
+// s = M q_n, w = cof(M) q_n, det M and the material products.  PACKED writes layout 4 (ids in
+// 21 bits each, no det M, materials into cmat), otherwise layout 3.
+template <bool PACKED>
 __global__ void k_pack_factored(const TetRec* __restrict__ rec, const int* __restrict__ inc_tet,
                                 const int* __restrict__ inc_vertex, int4* __restrict__ crec,
-                                int ninc) {
+                                float2* __restrict__ cmat, int ninc) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ninc) return;
     const TetRec r = rec[inc_tet[j]];
@@ -1082,6 +1155,14 @@ __global__ void k_pack_factored(const TetRec* __restrict__ rec, const int* __res
     }
     const float detm = M[0][0] * cof[0][0] + M[0][1] * cof[0][1] + M[0][2] * cof[0][2];
     const float a = r.c.y * r.c.z, b = r.c.y * r.c.w;
+    if (PACKED) {
+        const unsigned lo = (unsigned)nb[0] | ((unsigned)nb[1] << kPackedIdBits);
+        const unsigned hi = ((unsigned)nb[1] >> (32 - kPackedIdBits)) | ((unsigned)nb[2] << (2 * kPackedIdBits - 32));
+        crec[2 * j] = make_int4((int)lo, (int)hi, __float_as_int(sv[0]), __float_as_int(sv[1]));
+        crec[2 * j + 1] = make_int4(__float_as_int(sv[2]), __float_as_int(wv[0]), __float_as_int(wv[1]), __float_as_int(wv[2]));
+        cmat[j] = make_float2(a, b);
+        return;
+    }
     crec[3 * j] = make_int4(nb[0] | (n << 30), nb[1], nb[2], __float_as_int(sv[0]));
     crec[3 * j + 1] = make_int4(__float_as_int(sv[1]), __float_as_int(sv[2]), __float_as_int(wv[0]), __float_as_int(wv[1]));
     crec[3 * j + 2] = make_int4(__float_as_int(wv[2]), __float_as_int(detm), __float_as_int(a), __float_as_int(b));
@@ -1259,8 +1340,12 @@ template <> struct AdjElem<2> {
     __device__ __forceinline__ static Rec fetch(const AdjParams& p, int j) { return load_compact(p.crec, p.cmat, j); }
 };
 template <> struct AdjElem<3> {
-    using Rec = FactRec;
+    using Rec = FactRaw3;
     __device__ __forceinline__ static Rec fetch(const AdjParams& p, int j) { return load_fact(p.crec, j); }
+};
+template <> struct AdjElem<4> {
+    using Rec = FactRaw4;
+    __device__ __forceinline__ static Rec fetch(const AdjParams& p, int j) { return load_fact_packed(p.crec, p.cmat, j); }
 };
 
 // Adjoint element terms from a factored record (F = D M, dF = L M with L = [lam_0 lam_1 lam_2]):
@@ -1336,8 +1421,8 @@ __global__ void __launch_bounds__(256) k_adj_sweep(AdjParams p) {
     for (; j < j1; j += LANES) {
         const typename AdjElem<LAYOUT>::Rec r = nxt;
         if (j + LANES < j1) nxt = AdjElem<LAYOUT>::fetch(p, j + LANES);
-        if constexpr (LAYOUT == 3) {
-            fact_adjoint(r, xi, p.X, p.lam, acc);
+        if constexpr (LAYOUT >= 3) {
+            fact_adjoint(decode_fact(r), xi, p.X, p.lam, acc);
             continue;
         } else {
         const ElemView e = view_of(r, v);

@@ -72,7 +72,8 @@ template <int L> static SweepFn pick_sweep(int layout, bool prefetch) {
         case 0: return prefetch ? &k_sweep<L, 0, true> : &k_sweep<L, 0, false>;
         case 1: return prefetch ? &k_sweep<L, 1, true> : &k_sweep<L, 1, false>;
         case 2: return prefetch ? &k_sweep<L, 2, true> : &k_sweep<L, 2, false>;
-        default: return prefetch ? &k_sweep<L, 3, true> : &k_sweep<L, 3, false>;
+        case 3: return prefetch ? &k_sweep<L, 3, true> : &k_sweep<L, 3, false>;
+        default: return prefetch ? &k_sweep<L, 4, true> : &k_sweep<L, 4, false>;
     }
 }
 
@@ -84,6 +85,26 @@ static SweepFn pick_sweep(int lanes, int layout, bool prefetch) {
         case 8: return pick_sweep<8>(layout, prefetch);
         case 16: return pick_sweep<16>(layout, prefetch);
         default: return pick_sweep<32>(layout, prefetch);
+    }
+}
+
+template <int L> static void (*pick_persistent(int layout))(PersistParams) {
+    switch (layout) {
+        case 0: return &k_persistent<L, 0>;
+        case 1: return &k_persistent<L, 1>;
+        case 2: return &k_persistent<L, 2>;
+        case 3: return &k_persistent<L, 3>;
+        default: return &k_persistent<L, 4>;
+    }
+}
+
+// The adjoint reads tet records (layouts 0 and 1) or the forward's streamed incidence records.
+template <int L> static void (*pick_adj_sweep(int layout))(AdjParams) {
+    switch (layout) {
+        case 2: return &k_adj_sweep<L, 2>;
+        case 3: return &k_adj_sweep<L, 3>;
+        case 4: return &k_adj_sweep<L, 4>;
+        default: return &k_adj_sweep<L, 0>;
     }
 }
 
@@ -132,6 +153,7 @@ struct vbd_solver {
     // each vertex's dependent chain (the 2,673-vertex beam: 24.7 / 19.3 / 17.2 ms per 30 steps
     // with 4 / 8 / 16 lanes).
     bool lanes_auto = true;
+    bool layout_auto = true;  // layout 4 when the ids fit its 21-bit fields, else 3 (at init)
     // VBD_OPT_L2_PREFETCH: each colour sweep prefetches the next colour's streamed records into L2.
     // Off by default: on the 64^3 cube it measured 5.48 against 4.78 ms/step (the extra DRAM
     // traffic competes with the running colour's own stream).
@@ -229,12 +251,13 @@ struct vbd_solver {
         vbd::SweepParams p{xr,     xn,     pp.p,     y.p, inc_off.p, inc_tet.p, rec.p,          irec.p,
                            crec.p, cmat.p, status.p, vb,  ve,        dtsr,      omega, accel ? 1 : 0,
                            keep_pp ? 1 : 0, nullptr};
-        if (l2_prefetch && (layout == 2 || layout == 3) && crec.p && C > 0) {
+        if (l2_prefetch && layout >= 2 && crec.p && C > 0) {
             // the colour swept after this one (colour 0 of the next iteration after the last)
             const int cn = (c + 1) % C;
             const long long j0 = colour_inc[cn], j1 = colour_inc[cn + 1];
-            p.l2_next = reinterpret_cast<const char*>(crec.p + 3 * j0);
-            p.l2_bytes = (unsigned long long)(j1 - j0) * 48ull;
+            const int words = layout == 4 ? 2 : 3;  // int4 per incidence in crec
+            p.l2_next = reinterpret_cast<const char*>(crec.p + words * j0);
+            p.l2_bytes = (unsigned long long)(j1 - j0) * 16ull * words;
         }
         long long threads = (long long)(ve - vb) * lanes;
         vbd::SweepFn fn = vbd::pick_sweep(lanes, layout, prefetch != 0);
@@ -351,23 +374,11 @@ struct vbd_solver {
         }
         const int L = lanes < 4 ? 4 : lanes;
         void (*fn)(vbd::PersistParams) = nullptr;
-        switch (L * 4 + layout) {
-            case 16: fn = &vbd::k_persistent<4, 0>; break;
-            case 17: fn = &vbd::k_persistent<4, 1>; break;
-            case 18: fn = &vbd::k_persistent<4, 2>; break;
-            case 19: fn = &vbd::k_persistent<4, 3>; break;
-            case 32: fn = &vbd::k_persistent<8, 0>; break;
-            case 33: fn = &vbd::k_persistent<8, 1>; break;
-            case 34: fn = &vbd::k_persistent<8, 2>; break;
-            case 35: fn = &vbd::k_persistent<8, 3>; break;
-            case 64: fn = &vbd::k_persistent<16, 0>; break;
-            case 65: fn = &vbd::k_persistent<16, 1>; break;
-            case 66: fn = &vbd::k_persistent<16, 2>; break;
-            case 67: fn = &vbd::k_persistent<16, 3>; break;
-            case 128: fn = &vbd::k_persistent<32, 0>; break;
-            case 129: fn = &vbd::k_persistent<32, 1>; break;
-            case 130: fn = &vbd::k_persistent<32, 2>; break;
-            default: fn = &vbd::k_persistent<32, 3>; break;
+        switch (L) {
+            case 4: fn = vbd::pick_persistent<4>(layout); break;
+            case 8: fn = vbd::pick_persistent<8>(layout); break;
+            case 16: fn = vbd::pick_persistent<16>(layout); break;
+            default: fn = vbd::pick_persistent<32>(layout); break;
         }
         int per_sm = 0, sms = 0;
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0));
@@ -472,26 +483,18 @@ struct vbd_solver {
             vbd::AdjParams ap{X,         lr,      adj_G.p, y.p,   inc_off.p,     inc_tet.p,     rec.p,
                               crec.p,    cmat.p,  t.dtsr,  0,     0,             lo,            adj_lpp.p,
                               omega,     blend ? 1 : 0,    accel ? 1 : 0};
-            const int alay = (layout == 2 || layout == 3) ? layout : 0;
+            const int alay = layout >= 2 ? layout : 0;
             for (int k = 0; k < C; ++k) {
                 const int col = (adj_alternate && (it % 2 == 0)) ? C - 1 - k : k;
                 ap.v_begin = cstart[col];
                 ap.v_end = cstart[col + 1];
                 if (ap.v_end <= ap.v_begin) continue;
                 void (*fn)(vbd::AdjParams) = nullptr;
-                switch (L * 4 + alay) {
-                    case 16: fn = &vbd::k_adj_sweep<4, 0>; break;
-                    case 18: fn = &vbd::k_adj_sweep<4, 2>; break;
-                    case 19: fn = &vbd::k_adj_sweep<4, 3>; break;
-                    case 32: fn = &vbd::k_adj_sweep<8, 0>; break;
-                    case 34: fn = &vbd::k_adj_sweep<8, 2>; break;
-                    case 35: fn = &vbd::k_adj_sweep<8, 3>; break;
-                    case 64: fn = &vbd::k_adj_sweep<16, 0>; break;
-                    case 66: fn = &vbd::k_adj_sweep<16, 2>; break;
-                    case 67: fn = &vbd::k_adj_sweep<16, 3>; break;
-                    case 128: fn = &vbd::k_adj_sweep<32, 0>; break;
-                    case 130: fn = &vbd::k_adj_sweep<32, 2>; break;
-                    default: fn = &vbd::k_adj_sweep<32, 3>; break;
+                switch (L) {
+                    case 4: fn = vbd::pick_adj_sweep<4>(alay); break;
+                    case 8: fn = vbd::pick_adj_sweep<8>(alay); break;
+                    case 16: fn = vbd::pick_adj_sweep<16>(alay); break;
+                    default: fn = vbd::pick_adj_sweep<32>(alay); break;
                 }
                 cudaLaunchConfig_t cfg = {};
                 cfg.gridDim = dim3(vbd::nblk((long long)(ap.v_end - ap.v_begin) * L, 128));
@@ -616,11 +619,11 @@ struct vbd_solver {
             drop_graphs();
             irec.release();
         }
-        if (layout != 2 && cmat.p) {
+        if (layout != 2 && layout != 4 && cmat.p) {
             drop_graphs();
             cmat.release();
         }
-        if (layout != 2 && layout != 3 && crec.p) {
+        if (layout < 2 && crec.p) {
             drop_graphs();
             crec.release();
         }
@@ -633,12 +636,13 @@ struct vbd_solver {
                 vbd::k_pack_stream<<<vbd::nblk(ninc, 256), 256, 0, stream>>>(rec.p, inc_tet.p, irec.p, (int)ninc);
                 VBD_TRY(check_launch());
             }
-        } else if (layout == 2 || layout == 3) {
-            if (crec.n != 3 * (size_t)ninc) {
+        } else if (layout >= 2) {
+            const size_t words = layout == 4 ? 2 : 3;
+            if (crec.n != words * (size_t)ninc) {
                 drop_graphs();
-                VBD_TRY(crec.alloc(3 * (size_t)ninc));
+                VBD_TRY(crec.alloc(words * (size_t)ninc));
             }
-            if (layout == 2 && cmat.n != (size_t)ninc) {
+            if (layout != 3 && cmat.n != (size_t)ninc) {
                 drop_graphs();
                 VBD_TRY(cmat.alloc(ninc));
             }
@@ -646,9 +650,13 @@ struct vbd_solver {
                 vbd::k_pack_compact<<<vbd::nblk(ninc, 256), 256, 0, stream>>>(rec.p, inc_tet.p, inc_vertex.p, crec.p,
                                                                              cmat.p, (int)ninc);
                 VBD_TRY(check_launch());
+            } else if (ninc > 0 && layout == 3) {
+                vbd::k_pack_factored<false><<<vbd::nblk(ninc, 256), 256, 0, stream>>>(
+                    rec.p, inc_tet.p, inc_vertex.p, crec.p, nullptr, (int)ninc);
+                VBD_TRY(check_launch());
             } else if (ninc > 0) {
-                vbd::k_pack_factored<<<vbd::nblk(ninc, 256), 256, 0, stream>>>(rec.p, inc_tet.p, inc_vertex.p, crec.p,
-                                                                              (int)ninc);
+                vbd::k_pack_factored<true><<<vbd::nblk(ninc, 256), 256, 0, stream>>>(
+                    rec.p, inc_tet.p, inc_vertex.p, crec.p, cmat.p, (int)ninc);
                 VBD_TRY(check_launch());
             }
         }
@@ -742,6 +750,8 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     if ((tet_mu == nullptr) != (tet_lambda == nullptr))
         VBD_FAIL(VBD_ERR_INVALID_ARG, "give both tet_mu and tet_lambda, or neither");
     if ((long long)T * 4 > 0x7fffffffLL) VBD_FAIL(VBD_ERR_INVALID_ARG, "too many tets for 32-bit incidence ids");
+    if (!s->layout_auto && s->layout == 4 && N > vbd::kPackedMaxVertices)
+        VBD_FAIL(VBD_ERR_INVALID_ARG, "layout 4 holds vertex ids below 2^21; this mesh has %d vertices", N);
     VBD_TRY(vbd::check_tets(N, T, tets));
     // colour groups: a partition of the vertices into independent sets
     if (num_colours == 0 || group_offsets[0] != 0 || group_offsets[num_colours] != N)
@@ -867,6 +877,7 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
         while (L < 16 && largest * L * 2 <= (long long)sms * 1024) L *= 2;
         s->lanes = L;
     }
+    if (s->layout_auto) s->layout = N <= vbd::kPackedMaxVertices ? 4 : 3;
     s->colour_inc.assign(num_colours + 1, 0);
     for (int c = 0; c <= num_colours; ++c) s->colour_inc[c] = inc_off[cstart[c]];
     s->colour_bytes.assign(num_colours, 0.0);
@@ -1338,8 +1349,11 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
             s->block = value;
             return VBD_OK;
         case VBD_OPT_LAYOUT:
-            if (value < 0 || value > 3) VBD_FAIL(VBD_ERR_INVALID_ARG, "layout must be 0, 1, 2 or 3");
+            if (value < 0 || value > 4) VBD_FAIL(VBD_ERR_INVALID_ARG, "layout must be 0, 1, 2, 3 or 4");
+            if (value == 4 && s->ready && s->N > vbd::kPackedMaxVertices)
+                VBD_FAIL(VBD_ERR_INVALID_ARG, "layout 4 holds vertex ids below 2^21; this mesh has %d vertices", s->N);
             s->layout = value;
+            s->layout_auto = false;
             if (s->ready) {
                 VBD_TRY(s->repack_stream());
                 CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -1423,6 +1437,7 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
         int lanes, layout, prefetch, pdl, block;
     };
     static const Cand cands[] = {
+        {8, 4, 1, 1, 64}, {8, 4, 1, 1, 128}, {4, 4, 1, 1, 128}, {16, 4, 1, 1, 64}, {8, 4, 0, 1, 64},
         {8, 3, 1, 1, 64}, {8, 3, 1, 1, 128}, {4, 3, 1, 1, 128}, {16, 3, 1, 1, 64}, {8, 3, 0, 1, 64},
         {8, 3, 1, 0, 64}, {4, 2, 1, 1, 128}, {8, 2, 1, 1, 64},  {2, 2, 1, 1, 128}, {8, 1, 1, 1, 128},
         {8, 0, 1, 1, 128}, {4, 0, 1, 1, 128},
@@ -1432,9 +1447,10 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
     float best_ms = 1e30f;
-    Cand best = cands[0];
+    Cand best = {s->lanes, s->layout, s->prefetch, s->pdl, s->block};
     int rc = VBD_OK;
     for (const Cand& c : cands) {
+        if (c.layout == 4 && s->N > vbd::kPackedMaxVertices) continue;
         s->lanes = c.lanes;
         s->prefetch = c.prefetch;
         s->pdl = c.pdl;
