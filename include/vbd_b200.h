@@ -253,12 +253,16 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *                            meshes of at most 2^21 vertices only (VBD_ERR_INVALID_ARG otherwise)
  *                        Until it is set, vbd_solver_init picks layout 4 when the mesh has at most
  *                        2^21 vertices, else 3.
- *                        Defaults: 64-thread blocks, prefetch, PDL, graphs; lanes and layout
+ *                        Defaults: 64-thread blocks, PDL, graphs; lanes, layout and prefetch
  *                        chosen by vbd_solver_init.
  *   VBD_OPT_GRAPH:       1 = replay a captured CUDA graph per step, 0 = direct launches
  *   VBD_OPT_KERNEL_TIMING: 1 = launch directly and bracket every colour-sweep kernel with a CUDA
  *                        event pair on the handle's stream (read with vbd_solver_kernel_time)
- *   VBD_OPT_PREFETCH:    1 = load the next element record while evaluating the current one
+ *   VBD_OPT_PREFETCH:    0 = load each element record where it is used, 1 = load the next record
+ *                        while evaluating the current one, 2 = load a lane's first three records
+ *                        before the sweep's dependency wait (layouts 3 and 4; others run 1).  Until
+ *                        it is set: 2 with layout 4 when no lane holds more than three records
+ *                        (most incident tets of a free vertex / lanes), else 1.  All give the same bits
  *   VBD_OPT_PDL:         1 = launch colour sweeps with programmatic dependent launch, so a sweep
  *                        loads its element data while the previous sweep drains
  *   VBD_OPT_BLOCK:       threads per block of the sweep kernel: 64, 128 or 256

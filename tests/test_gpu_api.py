@@ -273,12 +273,20 @@ def test_layout_switches_rebuild_captured_graphs(gpu_device):
 def test_lane_count_chosen_at_init(gpu_device):
     """Until VBD_OPT_LANES is set, init picks the lane count from the mesh: 8 for the 64^3 cube (mean
     valence 22.9, colours large enough to fill the GPU), 16 for a small mesh that leaves SMs idle,
-    and an explicit setting sticks."""
+    and an explicit setting sticks.  The record prefetch follows: the deep one (2) when no lane holds
+    more than three records, else 1, unless VBD_OPT_PREFETCH is set."""
     from vbd_tetmesh_b200 import _capi
 
     cube = build_solver(meshgen.cube(64))
     assert cube.get_option(_capi.OPT_LANES) == 8
+    # at most 24 incident tets over 8 lanes: every lane's records fit the deep prefetch
+    assert cube.get_option(_capi.OPT_PREFETCH) == 2
     cube.close()
+    four = build_solver(meshgen.cube(6), lanes=4)
+    assert four.get_option(_capi.OPT_PREFETCH) == 1
+    four.set_option(_capi.OPT_PREFETCH, 2)
+    assert four.get_option(_capi.OPT_PREFETCH) == 2
+    four.close()
     small = build_solver(meshgen.beam())
     assert small.get_option(_capi.OPT_LANES) == 16
     small.close()

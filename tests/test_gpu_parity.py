@@ -151,6 +151,19 @@ def test_initial_velocity_and_stiff_material(gpu_device, seed):
     assert abs(ip32 - ip64) <= STIFF_IP_TOL_F64 * abs(ip64)
 
 
+@pytest.mark.parametrize("layout,lanes", [(3, 8), (4, 8), (4, 4), (4, 16)])
+def test_deep_prefetch_bit_identical(gpu_device, layout, lanes):
+    """VBD_OPT_PREFETCH 2 loads a lane's first three records before the dependency wait and any
+    further ones where they are used (4 lanes hold up to six on the cube); the summation order is
+    unchanged, so positions equal those of prefetch 0 and 1 bit for bit."""
+    m = meshgen.cube(12)
+    s = meshgen.CUBE_SETTINGS
+    out = [gpu_simulate(m, 2, s["dt"], s["iterations"], s["gravity"], True, s["rho"], layout=layout, lanes=lanes,
+                        options={_capi.OPT_PREFETCH: pf})["x"] for pf in (2, 1, 0)]
+    np.testing.assert_array_equal(out[0], out[1])
+    np.testing.assert_array_equal(out[0], out[2])
+
+
 def test_l2_prefetch_option_changes_no_result(gpu_device):
     """VBD_OPT_L2_PREFETCH only warms L2 with the next colour's records: bit-identical results."""
     m = meshgen.cube(12)

@@ -488,6 +488,9 @@ template <> struct Elem<4> {
 //   PREFETCH : the next element record is loaded while the current one is evaluated
 //   COHERENT : positions read with coherent loads (persistent kernel)
 // `nxt` holds the lane's first record if PREFETCH (fetched by the caller).
+template <int LANES>
+__device__ __forceinline__ void vertex_solve(const SweepParams& p, int v, int lane, bool active, float4 xi, Acc& acc);
+
 template <int LANES, int LAYOUT, bool PREFETCH, bool COHERENT>
 __device__ __forceinline__ void vertex_update(const SweepParams& p, int v, int lane, bool active, int j, int j1,
                                               typename Elem<LAYOUT>::Rec nxt) {
@@ -504,6 +507,13 @@ __device__ __forceinline__ void vertex_update(const SweepParams& p, int v, int l
         }
         Elem<LAYOUT>::template contrib<COHERENT>(r, v, xi, p.x, acc);
     }
+    vertex_solve<LANES>(p, v, lane, active, xi, acc);
+}
+
+// The group's reduction and the first lane's block solve, Chebyshev blend and stores (the second
+// half of vertex_update).
+template <int LANES>
+__device__ __forceinline__ void vertex_solve(const SweepParams& p, int v, int lane, bool active, float4 xi, Acc& acc) {
     group_reduce<LANES>(acc);
     if (!active || lane != 0) return;
 
@@ -565,9 +575,15 @@ __device__ __forceinline__ void l2_prefetch_share(const char* base, unsigned lon
 }
 
 // One colour of one Gauss-Seidel sweep per launch (VBDsolver::solve, VBD.cpp:114-158).  Element
-// data never changes during a sweep, so the lane's first record is fetched before the dependency
-// wait; positions are read only after it.
-template <int LANES, int LAYOUT, bool PREFETCH>
+// data never changes during a sweep, so records are fetched before the dependency wait; positions
+// are read only after it.
+//   PREFETCH 0: records are loaded where they are used
+//   PREFETCH 1: the lane's first record before the wait, then one record ahead
+//   PREFETCH k >= 2: the lane's first k records before the wait, any further ones where used, so a
+//            lane with at most k records pays no DRAM round trip after the wait; same summation
+//            order, so the same bits as PREFETCH 1.  (Keeping k records in flight past the first k,
+//            as a ring, took 70-80 registers and ran slower.)
+template <int LANES, int LAYOUT, int PREFETCH>
 __global__ void __launch_bounds__(256) k_sweep(SweepParams p) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = LANES == 1 ? 0 : (threadIdx.x & (LANES - 1));
@@ -579,12 +595,31 @@ __global__ void __launch_bounds__(256) k_sweep(SweepParams p) {
         j1 = __ldg(p.inc_off + v + 1);
     }
     const int j = j0 + lane;
-    typename Elem<LAYOUT>::Rec nxt;
-    if (PREFETCH && j < j1) nxt = Elem<LAYOUT>::fetch(p, j);
-    if (p.l2_bytes && threadIdx.x == 0) l2_prefetch_share(p.l2_next, p.l2_bytes);
-    pdl_trigger();
-    pdl_wait();
-    vertex_update<LANES, LAYOUT, PREFETCH, false>(p, v, lane, active, j, j1, nxt);
+    if constexpr (PREFETCH >= 2) {
+        typename Elem<LAYOUT>::Rec buf[PREFETCH];
+#pragma unroll
+        for (int k = 0; k < PREFETCH; ++k)
+            if (j + k * LANES < j1) buf[k] = Elem<LAYOUT>::fetch(p, j + k * LANES);
+        if (p.l2_bytes && threadIdx.x == 0) l2_prefetch_share(p.l2_next, p.l2_bytes);
+        pdl_trigger();
+        pdl_wait();
+        const float4 xi = active ? p.x[v] : make_float4(0.f, 0.f, 0.f, 0.f);
+        Acc acc;
+        acc.zero();
+#pragma unroll
+        for (int k = 0; k < PREFETCH; ++k)
+            if (j + k * LANES < j1) Elem<LAYOUT>::template contrib<false>(buf[k], v, xi, p.x, acc);
+        for (int jj = j + PREFETCH * LANES; jj < j1; jj += LANES)
+            Elem<LAYOUT>::template contrib<false>(Elem<LAYOUT>::fetch(p, jj), v, xi, p.x, acc);
+        vertex_solve<LANES>(p, v, lane, active, xi, acc);
+    } else {
+        typename Elem<LAYOUT>::Rec nxt;
+        if (PREFETCH && j < j1) nxt = Elem<LAYOUT>::fetch(p, j);
+        if (p.l2_bytes && threadIdx.x == 0) l2_prefetch_share(p.l2_next, p.l2_bytes);
+        pdl_trigger();
+        pdl_wait();
+        vertex_update<LANES, LAYOUT, PREFETCH != 0, false>(p, v, lane, active, j, j1, nxt);
+    }
 }
 
 // ---- VBD_GPU_Solver semantics (the reference's GPU wrapper) ------------------------------------

@@ -67,17 +67,25 @@ static float omega_of_wrapper(int order, float rho, float prev) {
 
 using SweepFn = void (*)(SweepParams);
 
-template <int L> static SweepFn pick_sweep(int layout, bool prefetch) {
+// prefetch 0 / 1 / 2 = k_sweep's PREFETCH 0 / 1 / 3 (deep prefetch for the factored layouts only;
+// the others run PREFETCH 1 for option 2).
+template <int L, int LAYOUT> static SweepFn pick_depth(int prefetch) {
+    if (prefetch == 0) return &k_sweep<L, LAYOUT, 0>;
+    if (prefetch == 1 || LAYOUT < 3) return &k_sweep<L, LAYOUT, 1>;
+    return &k_sweep<L, LAYOUT, (LAYOUT < 3 ? 1 : 3)>;
+}
+
+template <int L> static SweepFn pick_sweep(int layout, int prefetch) {
     switch (layout) {
-        case 0: return prefetch ? &k_sweep<L, 0, true> : &k_sweep<L, 0, false>;
-        case 1: return prefetch ? &k_sweep<L, 1, true> : &k_sweep<L, 1, false>;
-        case 2: return prefetch ? &k_sweep<L, 2, true> : &k_sweep<L, 2, false>;
-        case 3: return prefetch ? &k_sweep<L, 3, true> : &k_sweep<L, 3, false>;
-        default: return prefetch ? &k_sweep<L, 4, true> : &k_sweep<L, 4, false>;
+        case 0: return pick_depth<L, 0>(prefetch);
+        case 1: return pick_depth<L, 1>(prefetch);
+        case 2: return pick_depth<L, 2>(prefetch);
+        case 3: return pick_depth<L, 3>(prefetch);
+        default: return pick_depth<L, 4>(prefetch);
     }
 }
 
-static SweepFn pick_sweep(int lanes, int layout, bool prefetch) {
+static SweepFn pick_sweep(int lanes, int layout, int prefetch) {
     switch (lanes) {
         case 1: return pick_sweep<1>(layout, prefetch);
         case 2: return pick_sweep<2>(layout, prefetch);
@@ -154,6 +162,8 @@ struct vbd_solver {
     // with 4 / 8 / 16 lanes).
     bool lanes_auto = true;
     bool layout_auto = true;  // layout 4 when the ids fit its 21-bit fields, else 3 (at init)
+    bool prefetch_auto = true;  // see eff_prefetch
+    int max_valence = 0;        // most incident tets of any free vertex
     // VBD_OPT_L2_PREFETCH: each colour sweep prefetches the next colour's streamed records into L2.
     // Off by default: on the 64^3 cube it measured 5.48 against 4.78 ms/step (the extra DRAM
     // traffic competes with the running colour's own stream).
@@ -238,6 +248,15 @@ struct vbd_solver {
         graphs.clear();
     }
 
+    // The record prefetch the sweeps run.  Until VBD_OPT_PREFETCH is set: 2 (the lane's first three
+    // records before the dependency wait) with the packed records when no lane holds more than
+    // three records, else 1.  Measured on the 64^3 cube (8 lanes, at most 3 records a lane): 4.46
+    // against 4.55 ms/step; on the 512-mesh batch (4 lanes, up to 6): 7.72 against 7.44.
+    int eff_prefetch() const {
+        if (!prefetch_auto) return prefetch;
+        return (layout == 4 && lanes > 0 && (max_valence + lanes - 1) / lanes <= 3) ? 2 : 1;
+    }
+
     int check_launch() {
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) VBD_FAIL(VBD_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
@@ -260,7 +279,7 @@ struct vbd_solver {
             p.l2_bytes = (unsigned long long)(j1 - j0) * 16ull * words;
         }
         long long threads = (long long)(ve - vb) * lanes;
-        vbd::SweepFn fn = vbd::pick_sweep(lanes, layout, prefetch != 0);
+        vbd::SweepFn fn = vbd::pick_sweep(lanes, layout, eff_prefetch());
         int threads_per_block = block;
         if (semantics) threads = (long long)(ve - vb) * vbd::kWrapperLanes;
         cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -444,7 +463,7 @@ struct vbd_solver {
         key.accel = t.accel;
         key.lanes = lanes;
         key.layout = layout;
-        key.prefetch = prefetch;
+        key.prefetch = eff_prefetch();
         key.pdl = pdl;
         key.block = block;
         key.semantics = semantics;
@@ -878,6 +897,8 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
         s->lanes = L;
     }
     if (s->layout_auto) s->layout = N <= vbd::kPackedMaxVertices ? 4 : 3;
+    s->max_valence = 0;
+    for (int i = 0; i < nfree; ++i) s->max_valence = std::max(s->max_valence, inc_off[i + 1] - inc_off[i]);
     s->colour_inc.assign(num_colours + 1, 0);
     for (int c = 0; c <= num_colours; ++c) s->colour_inc[c] = inc_off[cstart[c]];
     s->colour_bytes.assign(num_colours, 0.0);
@@ -1046,7 +1067,7 @@ int vbd_solver_solve(vbd_solver* s, int32_t iterations, float dt_sqr_reciprocal,
     key.init = init_mode;
     key.lanes = s->lanes;
     key.layout = s->layout;
-    key.prefetch = s->prefetch;
+    key.prefetch = s->eff_prefetch();
     key.pdl = s->pdl;
     key.block = s->block;
     key.semantics = s->semantics;
@@ -1090,7 +1111,7 @@ int vbd_solver_step(vbd_solver* s, float dt, int32_t substeps, int32_t iteration
     key.accel = use_acceleration ? 1 : 0;
     key.lanes = s->lanes;
     key.layout = s->layout;
-    key.prefetch = s->prefetch;
+    key.prefetch = s->eff_prefetch();
     key.pdl = s->pdl;
     key.block = s->block;
     key.semantics = s->semantics;
@@ -1319,7 +1340,9 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
             s->lanes_auto = false;
             return VBD_OK;
         case VBD_OPT_PREFETCH:
-            s->prefetch = value ? 1 : 0;
+            if (value < 0 || value > 2) VBD_FAIL(VBD_ERR_INVALID_ARG, "prefetch must be 0, 1 or 2");
+            s->prefetch = value;
+            s->prefetch_auto = false;
             return VBD_OK;
         case VBD_OPT_PDL:
             s->pdl = value ? 1 : 0;
@@ -1378,7 +1401,7 @@ int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value) {
         case VBD_OPT_LAYOUT: *value = s->layout; return VBD_OK;
         case VBD_OPT_GRAPH: *value = s->use_graph; return VBD_OK;
         case VBD_OPT_KERNEL_TIMING: *value = s->timing; return VBD_OK;
-        case VBD_OPT_PREFETCH: *value = s->prefetch; return VBD_OK;
+        case VBD_OPT_PREFETCH: *value = s->eff_prefetch(); return VBD_OK;
         case VBD_OPT_PDL: *value = s->pdl; return VBD_OK;
         case VBD_OPT_BLOCK: *value = s->block; return VBD_OK;
         case VBD_OPT_PERSISTENT: *value = s->persistent; return VBD_OK;
@@ -1437,7 +1460,8 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
         int lanes, layout, prefetch, pdl, block;
     };
     static const Cand cands[] = {
-        {8, 4, 1, 1, 64}, {8, 4, 1, 1, 128}, {4, 4, 1, 1, 128}, {16, 4, 1, 1, 64}, {8, 4, 0, 1, 64},
+        {8, 4, 2, 1, 64}, {8, 4, 1, 1, 64}, {8, 4, 1, 1, 128}, {4, 4, 1, 1, 128}, {16, 4, 2, 1, 64},
+        {16, 4, 1, 1, 64}, {8, 4, 0, 1, 64},
         {8, 3, 1, 1, 64}, {8, 3, 1, 1, 128}, {4, 3, 1, 1, 128}, {16, 3, 1, 1, 64}, {8, 3, 0, 1, 64},
         {8, 3, 1, 0, 64}, {4, 2, 1, 1, 128}, {8, 2, 1, 1, 64},  {2, 2, 1, 1, 128}, {8, 1, 1, 1, 128},
         {8, 0, 1, 1, 128}, {4, 0, 1, 1, 128},
@@ -1447,7 +1471,8 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
     float best_ms = 1e30f;
-    Cand best = {s->lanes, s->layout, s->prefetch, s->pdl, s->block};
+    Cand best = {s->lanes, s->layout, s->eff_prefetch(), s->pdl, s->block};
+    s->prefetch_auto = false;
     int rc = VBD_OK;
     for (const Cand& c : cands) {
         if (c.layout == 4 && s->N > vbd::kPackedMaxVertices) continue;
