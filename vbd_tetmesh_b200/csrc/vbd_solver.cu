@@ -68,9 +68,11 @@ static float omega_of_wrapper(int order, float rho, float prev) {
 using SweepFn = void (*)(SweepParams);
 
 // prefetch 0 / 1 / 2 = k_sweep's PREFETCH 0 / 1 / 3 (deep prefetch for the factored layouts only;
-// the others run PREFETCH 1 for option 2).
+// the others run PREFETCH 1 for option 2).  The factored layouts' PREFETCH 1 runs as
+// k_sweep_capped (56 registers).
 template <int L, int LAYOUT> static SweepFn pick_depth(int prefetch) {
     if (prefetch == 0) return &k_sweep<L, LAYOUT, 0>;
+    if (LAYOUT >= 3 && L > 1 && prefetch == 1) return &k_sweep_capped<L, LAYOUT>;
     if (prefetch == 1 || LAYOUT < 3) return &k_sweep<L, LAYOUT, 1>;
     return &k_sweep<L, LAYOUT, (LAYOUT < 3 ? 1 : 3)>;
 }
@@ -251,7 +253,9 @@ struct vbd_solver {
     // The record prefetch the sweeps run.  Until VBD_OPT_PREFETCH is set: 2 (the lane's first three
     // records before the dependency wait) with the packed records when no lane holds more than
     // three records, else 1.  Measured on the 64^3 cube (8 lanes, at most 3 records a lane): 4.46
-    // against 4.55 ms/step; on the 512-mesh batch (4 lanes, up to 6): 7.72 against 7.44.
+    // against 4.55 ms/step; on the 512-mesh batch (4 lanes, up to 6): 7.72 against 7.44 (both
+    // before PREFETCH 1 was held to 56 registers, which brought the cube to 4.48 and the batch to
+    // 7.10).
     int eff_prefetch() const {
         if (!prefetch_auto) return prefetch;
         return (layout == 4 && lanes > 0 && (max_valence + lanes - 1) / lanes <= 3) ? 2 : 1;
