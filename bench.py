@@ -596,7 +596,18 @@ def main():
         e2e_value = units / e2e_max
 
     peak, peak_kind = measured_peaks()
-    achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9 if sweep_ms > 0 else None
+    # The sweep kernel's average launch duration in the timed region: the region's time (CUDA events
+    # on the solver's stream, max over ranks) over the sweep launches in it.  The predictor and
+    # velocity kernels (2 of 402 launches, 0.3% of the step's device time in the ncu launch list)
+    # are charged to the sweeps, so this bounds the sweep's bandwidth from below.  The second pass,
+    # one event pair around every sweep launched on its own (no graph, no PDL overlap), is reported
+    # beside it as "isolated".
+    achieved = iso_achieved = launch_us = None
+    if sweep_launches and sweep_ms > 0:
+        bytes_per_launch = sweep_bytes / sweep_launches
+        launch_us = ms_max * 1e3 / sweep_launches
+        achieved = bytes_per_launch / (launch_us * 1e-6) / 1e9
+        iso_achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9
     # DRAM traffic per launch: the ncu-measured traffic / algorithmic-bytes ratio of the sweep
     # kernel (profiles/sweep_cube64_dram.txt) times this run's algorithmic bytes per launch
     traffic = None
@@ -636,7 +647,14 @@ def main():
             "frac": (achieved / peak) if achieved else None,
             "traffic": traffic,
             "sweep_launches_timed": int(sweep_launches),
-            "sweep_ms_avg": sweep_ms / sweep_launches if sweep_launches else None,
+            "launch_us_in_timed_region": launch_us,
+            "alg_bytes_per_launch": (sweep_bytes / sweep_launches) if sweep_launches else None,
+            "isolated": {
+                "achieved": iso_achieved,
+                "frac": (iso_achieved / peak) if iso_achieved else None,
+                "launch_us": (sweep_ms * 1e3 / sweep_launches) if sweep_launches else None,
+                "how": "one CUDA event pair around every sweep launched on its own (no graph, no PDL overlap)",
+            },
             "alg_bytes_per_vertex_iteration": alg_bytes_per_vi,
             "step_frac_of_roofline": (value / world) * (alg_bytes_per_vi or 0) / (peak * 1e9),
         },
