@@ -12,10 +12,13 @@ E = 1e6 Pa, nu = 0.4, density 1000, bottom face pinned, seeded initial velocitie
   timed steps outside the timed events.
 * e2e: the same metric through the C ABI with host buffers: each step uploads positions and
   velocities from pinned host memory, steps, and reads both back.
-* roofline: the colour-sweep kernel, timed live with a CUDA event pair around every launch (a
-  second timed pass); algorithmic bytes = 60 B per incident tet + 96 B per swept vertex.
-* cpu_baseline (rank 0, N = 1): the oracle's reference-cost restatement (literal 12x12 element
-  Hessian per incidence, energy every 10 iterations) on all host cores, one cube iteration per sample.
+* roofline: the colour-sweep kernel (400 of a step's 402 launches): its algorithmic bytes per launch
+  (60 B per incident tet + 96 B per swept vertex) over the timed region's CUDA-event time per sweep
+  launch; a second pass with an event pair around every sweep launched on its own is reported
+  beside it as "isolated".
+* cpu_baseline (rank 0, N = 1): the reference's own CPU sources (oracle/_ref, compiled against the
+  Eigen-API subset) on all host cores, one cube iteration per sample; the oracle's reference-cost
+  restatement (literal 12x12 element Hessian, energy every 10 iterations) when they are not built.
 * --impl reference: that CPU implementation alone (rank 0), each step one cube iteration.
 * N > 1 (torchrun): one replica of the cube per GPU ("replicas only": a single mesh does not
   shard); no collective on the data path, barrier + max-over-ranks timing.
