@@ -31,6 +31,7 @@ import os
 import signal
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -61,6 +62,8 @@ def parse_args():
     ap.add_argument("--batch-steps", type=int, default=3)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-material-id", action="store_true")
+    ap.add_argument("--clocks-dir", default=None,
+                    help="directory for the raw nvidia-smi clock samples (default: a temporary directory)")
     return ap.parse_args()
 
 
@@ -147,15 +150,17 @@ class ClockSampler:
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_index):
+    def __init__(self, device_index, out_dir=None):
         self.device_index = device_index
+        self.out_dir = out_dir
         self.proc = None
         self.path = None
 
     def start(self):
         try:
-            os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-            self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{self.device_index}.csv")
+            out_dir = self.out_dir or tempfile.mkdtemp(prefix="vbd_bench_clocks_")
+            os.makedirs(out_dir, exist_ok=True)
+            self.path = os.path.join(out_dir, f"clocks_rank{self.device_index}.csv")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
                  "-lms", "20"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
@@ -533,7 +538,7 @@ def main():
 
     # nvidia-smi needs about a second to start sampling: launch it before the warm-up so that its
     # samples cover the timed passes
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(local, args.clocks_dir)
     clocks.start()
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):

@@ -182,8 +182,8 @@ def test_diff_beam_config_matches_fp64_adjoint_within_cost(gpu_device):
 def test_diff_beam_converged_matches_finite_differences(gpu_device):
     """With the forward converged (120 iterations per step) the implicit gradient is the derivative of
     the step map: the GPU adjoint matches central finite differences of the FP64 forward (eps 1e-4
-    relative) within 1e-3.  At the stated 30 iterations the forward map is not converged and the two
-    differ."""
+    relative) within 1e-3.  At the stated 30 iterations the forward map is not converged, so finite
+    differences of it differ from the implicit gradient by the unconverged part."""
     m, tip, target = meshgen.diff_beam()
     st = dict(meshgen.DIFF_SETTINGS, iterations=120)
     n = m.num_verts
