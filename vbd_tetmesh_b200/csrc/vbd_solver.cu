@@ -152,14 +152,14 @@ struct vbd_solver {
     vbd::DBuf<float> stage, mat_stage;
     vbd::DBuf<unsigned long long> status;
     vbd::DBuf<double> partials, scalar;
-    // defaults: the fastest shape measured on the 64^3 cube (compact streamed records, 4 lanes per
-    // vertex, record prefetch, programmatic dependent launch, 128-thread blocks)
+    // defaults: 64-thread blocks, programmatic dependent launch and graphs; lanes, layout and
+    // record prefetch are chosen at init from the mesh (below) until their options are set
     int lanes = 8, layout = 3, use_graph = 1, timing = 0, prefetch = 1, pdl = 1, block = 64;
     // Until VBD_OPT_LANES is set, init picks the lane count: 8 lanes when the free vertices average
     // at least 21 incident tets (the 64^3 cube: 22.9, 5.04 vs 5.49 ms/step with 4), else 4 (the
     // 512-block batch: 19.5, 9.06 vs 10.2 ms/step with 8); then doubled, up to 16, while the
-    // largest colour would still fill less than half of the GPU's resident threads (1024 per SM at
-    // this kernel's 64 registers): a small mesh leaves SMs idle, and more lanes per vertex shorten
+    // largest colour would still fill less than half of the GPU's resident threads (taken as 1024
+    // per SM, the sweep's occupancy at 60-64 registers): a small mesh leaves SMs idle, and more lanes per vertex shorten
     // each vertex's dependent chain (the 2,673-vertex beam: 24.7 / 19.3 / 17.2 ms per 30 steps
     // with 4 / 8 / 16 lanes).
     bool lanes_auto = true;
