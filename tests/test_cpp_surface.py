@@ -9,7 +9,9 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INC = ["-I", os.path.join(ROOT, "include", "vbd"), "-I", os.path.join(ROOT, "include")]
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
-REF_MAIN = "/root/reference/main.cpp"
+# main.cpp of the reference tree oracle/Makefile reads (its REF: VBD_REF_DIR or the recipe's default)
+REF_MAIN = os.path.join(subprocess.run(["make", "-s", "--no-print-directory", "-C", os.path.join(ROOT, "oracle"),
+                                        "print-ref"], capture_output=True, text=True).stdout.strip(), "main.cpp")
 
 
 def test_headers_compile(tmp_path):
