@@ -55,6 +55,37 @@ def test_noalloc_ip_matches_solver_energy_on_two_calls(gpu_device):
     s.close()
 
 
+def test_noalloc_bad_ids_flagged_then_next_call_clean(gpu_device):
+    """A tet holding an id outside [0, N) is skipped before any load and reported; the next call,
+    on the same scratch (its error flag still set by the failed call), clears the flag and matches
+    vbd_solver_energy."""
+    import torch
+
+    m = meshgen.jittered_block(6, 4, 4, seed=9, per_tet_sigma=0.2)
+    s = build_solver(m)
+    h = float(np.float32(1.0 / 60.0))
+    s.step(1.0 / 60.0, 8, (0.0, -9.8, 0.0), True, 0.9)
+    dm, v0 = precompute_tets(m.rest, m.tets)
+    bad = m.tets.copy()
+    bad[3, 2] = m.num_verts       # one past the end
+    bad[7, 0] = -5                # negative
+    args = [_dev(torch, a, np.float32) for a in (s.get_positions(), s.get_inertia(), s.vertex_mass)]
+    rest = [_dev(torch, dm.reshape(-1, 9), np.float32), _dev(torch, v0, np.float32), _dev(torch, m.mu, np.float32),
+            _dev(torch, m.lam, np.float32)]
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    tets_bad = _dev(torch, bad, np.int32)
+    with pytest.raises(VBDError) as e:
+        _capi.call("vbd_ip_energy_noalloc", m.num_verts, m.num_tets, *[a.data_ptr() for a in args],
+                   tets_bad.data_ptr(), *[a.data_ptr() for a in rest], h, out.data_ptr(), None)
+    assert e.value.code == 1 and f"outside [0, {m.num_verts})" in e.value.message
+    tets = _dev(torch, m.tets, np.int32)
+    _capi.call("vbd_ip_energy_noalloc", m.num_verts, m.num_tets, *[a.data_ptr() for a in args], tets.data_ptr(),
+               *[a.data_ptr() for a in rest], h, out.data_ptr(), None)
+    expected = s.energy(_capi.ENERGY_IP, h)
+    assert abs(float(out.cpu()[0]) - expected) <= IP_RTOL * abs(expected)
+    s.close()
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch(gpu_device):
     out = C.c_double(0.0)
     with pytest.raises(VBDError) as e:

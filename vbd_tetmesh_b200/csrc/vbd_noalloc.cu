@@ -13,7 +13,9 @@
 //   * The host never names the array as an address: at the first call on each device, with that
 //     device current, cudaGetSymbolAddress gives the device pointer, which is cached per device
 //     and passed to the kernels.  That first call therefore has to come before any stream
-//     capture on that device.
+//     capture on that device.  Later calls look the address up again whenever their stream is not
+//     capturing (a lookup allocates nothing), so a cudaDeviceReset between two calls, after which
+//     the array lives in a new context, is picked up by the next call.
 //   * Calls share the array and it keeps the last call's contents.  The error flag must start at
 //     zero and is cleared at the start of every call; each partial slot read in a call is written
 //     earlier in the same call.  Two calls whose work overlaps on the GPU (different streams, or
@@ -118,11 +120,20 @@ __global__ void __launch_bounds__(1024) k_ip_total(const double* __restrict__ sc
     }
 }
 
-// Device address of the scratch array on the current device (set up once per device).
-int scratch_address(int device, double** out) {
+// Device address of the scratch array on the current device: looked up at the first call on the
+// device (set-up), and again at later calls whose stream is not capturing.
+int scratch_address(int device, cudaStream_t stream, double** out) {
     if (device < 0 || device >= kMaxDevices) VBD_FAIL(VBD_ERR_NO_DEVICE, "device ordinal %d not supported", device);
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[device]) {
+    bool lookup = g_scratch_addr[device] == nullptr;
+    if (!lookup) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(stream, &cs) == cudaSuccess)
+            lookup = cs == cudaStreamCaptureStatusNone;
+        else
+            cudaGetLastError();  // the failed query's own error is not left for the caller to find
+    }
+    if (lookup) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess)
@@ -156,9 +167,9 @@ extern "C" int vbd_ip_energy_noalloc(int32_t num_verts, int32_t num_tets, const 
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) VBD_FAIL(VBD_ERR_NO_DEVICE, "no current CUDA device: %s", cudaGetErrorString(e));
-    double* scratch = nullptr;
-    if (int rc = scratch_address(device, &scratch)) return rc;
     cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    double* scratch = nullptr;
+    if (int rc = scratch_address(device, stream, &scratch)) return rc;
     const int nblocks = total > 0 ? (int)((total + kPerBlock - 1) / kPerBlock) : 1;
     e = cudaMemsetAsync(scratch + kFlagSlot, 0, sizeof(double), stream);
     if (e != cudaSuccess) VBD_FAIL(VBD_ERR_CUDA, "clearing the scratch flag failed: %s", cudaGetErrorString(e));
