@@ -137,6 +137,57 @@ def cpu_reference(mesh, samples, warmup=0):
     return mesh.num_verts * samples / total, threads, total, kind, what
 
 
+def cpu_restatement(cube_mesh):
+    """The oracle's reference-cost restatement of the reference CPU path (literal 12x12 element
+    Hessian per incidence, computeTotalEnergy every 10th iteration, VBD.cpp:60-203), race-free:
+    OpenMP within each colour, the same results at any thread count.  Timed at 1 thread and at all
+    host threads on
+      * the beam (16x4x4 cells, 425 vertices), 100 steps x 20 iterations in full, and
+      * the cube, one full step (50 iterations) at all threads; at 1 thread (about 8 s per
+        iteration) from one iteration without and one with the energy evaluation, extrapolated to
+        the step's 50 iterations and 5 energy evaluations.
+    Returns the runs in vertex-iterations/s."""
+    from oracle import pyoracle as po
+    from vbd_tetmesh_b200 import meshgen
+
+    allc = max(1, po.max_threads())
+    runs = []
+    beam, bs = meshgen.beam(), meshgen.BEAM_SETTINGS
+    for thr in (1, allc):
+        h = po.Handle(beam, po.LITERAL_FULL12, thr)
+        t0 = time.perf_counter()
+        h.step(100, bs["dt"], bs["iterations"], bs["gravity"], True, bs["rho"], energy=True)
+        t = time.perf_counter() - t0
+        h.close()
+        runs.append({"workload": "beam 16x4x4 cells (425 vertices), 100 steps x 20 iterations, in full",
+                     "threads": thr, "seconds": t, "value": beam.num_verts * 20 * 100 / t})
+    cs = meshgen.CUBE_SETTINGS
+    n = cube_mesh.num_verts
+    h = po.Handle(cube_mesh, po.LITERAL_FULL12, 1)
+    t0 = time.perf_counter()
+    h.step(1, cs["dt"], 1, cs["gravity"], True, cs["rho"], energy=False)
+    t_it = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    h.step(1, cs["dt"], 1, cs["gravity"], True, cs["rho"], energy=True)
+    t_en = max(time.perf_counter() - t0 - t_it, 0.0)
+    h.close()
+    t_step = 50 * t_it + 5 * t_en
+    runs.append({"workload": "cube 64^3 (274,625 vertices), one step of 50 iterations, extrapolated from one "
+                             "iteration without and one with the energy evaluation",
+                 "threads": 1, "seconds": t_step, "value": n * 50 / t_step, "measured_seconds": t_it + t_it + t_en})
+    h = po.Handle(cube_mesh, po.LITERAL_FULL12, allc)
+    t0 = time.perf_counter()
+    h.step(1, cs["dt"], 50, cs["gravity"], True, cs["rho"], energy=True)
+    t = time.perf_counter() - t0
+    h.close()
+    runs.append({"workload": "cube 64^3 (274,625 vertices), one full step of 50 iterations", "threads": allc,
+                 "seconds": t, "value": n * 50 / t})
+    return {"kind": "port", "unit": UNIT, "host_threads": allc,
+            "what": "the oracle's reference-cost restatement of VBDsolver::step: literal 12x12 element Hessian per "
+                    "incidence, computeTotalEnergy every 10th iteration, OpenMP within each colour (race-free)",
+            "runs": runs}
+
+
 def meshgen_settings():
     from vbd_tetmesh_b200 import meshgen
 
@@ -367,6 +418,13 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
         launches_b = (bs.kernel_launches() - l0) // (K + 1)
         xb = bs.get_positions()
         batch_lanes = bs.get_option(_capi.OPT_LANES)
+        # algorithmic bytes of one step's colour sweeps (60 B per incidence + 96 B per swept vertex),
+        # from a pass with an event pair around every sweep (after the positions were read)
+        bs.set_option(_capi.OPT_KERNEL_TIMING, 1)
+        bs.kernel_time(reset=True)
+        flush.fill_(1.0)
+        bs.step(dt, iters, g, True, rho)
+        sw_ms, sw_launches, sw_bytes = bs.kernel_time(reset=True)
         bs.close()
         # the per-mesh solvers use the batch solver's lane count, so each mesh's arithmetic (and
         # result) is the batch's
@@ -387,6 +445,29 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
                                                       dist, f"cuda:{local}")
     units = nverts * iters * K
     allm = meshgen.concat(meshes)
+    peak, peak_kind = measured_peaks()
+    step_s = ms_b / K * 1e-3
+    achieved = sw_bytes / step_s / 1e9 if sw_bytes else None
+    roofline = {
+        "bound": "hbm",
+        "kernel": "vbd::k_sweep (colour sweeps of all meshes, one launch per colour)",
+        "achieved": achieved,
+        "peak": peak,
+        "peak_source": peak_kind,
+        "unit": "GB/s",
+        "frac": achieved / peak if achieved else None,
+        "alg_bytes_per_step": sw_bytes,
+        "alg_bytes_per_vertex_iteration": sw_bytes / (b.num_verts * iters) if sw_bytes else None,
+        "sweep_launches_per_step": int(sw_launches),
+        "launch_us_in_timed_region": (ms_b / K * 1e3 / sw_launches) if sw_launches else None,
+        "how": "this rank's algorithmic sweep bytes of one step (60 B per incidence + 96 B per swept vertex) over "
+               "the timed region's device time per step; predictor and velocity kernels are charged to the sweeps",
+        "isolated": {
+            "achieved": sw_bytes / (sw_ms * 1e-3) / 1e9 if sw_ms else None,
+            "launch_us": sw_ms * 1e3 / sw_launches if sw_launches else None,
+            "how": "one CUDA event pair around every sweep launched on its own (no graph, no PDL overlap)",
+        },
+    }
     return {
         "workload": f"{len(meshes)} jittered grid blocks, dims U{{4..24}}^3 x 6 tets, E log-U[1e4,1e6], "
                     "nu U[0.2,0.45], one face pinned, dt 1/60, 20 iterations, Chebyshev 0.9 (assumed), seed 2024",
@@ -404,6 +485,7 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
         "plain_launches_per_step": int(launches_p),
         "bitwise_equal_to_plain": mism == 0.0,
         "sharding": f"whole meshes over {world} rank(s), balanced by tet count" if world > 1 else "single GPU",
+        "roofline": roofline,
     }
 
 
@@ -439,6 +521,18 @@ def bench_adjoint(local, stream):
             res.append((tf, tb))
         s.close()
     tf, tb = min(res, key=lambda r: r[1])
+    # Algorithmic bytes of the backward pass: the recomputed forward sweeps of the older segments
+    # (the newest segment's states are kept) at the forward's 60 B per incidence + 96 B per swept
+    # vertex, and the adjoint sweeps at 68 B per incidence (the record plus per-tet mu, lambda) +
+    # 128 B per swept vertex (x, lambda read / write, G, y, lambda before the previous sweep).
+    free = m.fixed == 0
+    inc_free = int(free[m.tets].sum())
+    nfree = int(free.sum())
+    recomputed = st["steps"] - min(st["checkpoint"], st["steps"])
+    fwd_iter = 60.0 * inc_free + 96.0 * nfree
+    adj_sweep = 68.0 * inc_free + 128.0 * nfree
+    alg = recomputed * st["iterations"] * fwd_iter + st["steps"] * st["adjoint_iterations"] * adj_sweep
+    peak, peak_kind = measured_peaks()
     return {
         "workload": "32x8x8 beam x 6 tets (2,673 vertices, 12,288 tets), per-tet log-normal mu/lambda (sigma 0.2), "
                     "30 steps x 30 iterations, Chebyshev 0.95, checkpoint every 10 steps, loss on 25 tip vertices",
@@ -448,6 +542,17 @@ def bench_adjoint(local, stream):
         "adjoint_sweeps_per_step": st["adjoint_iterations"],
         "adjoint_rho": st["adjoint_rho"],
         "accuracy": "checked in tests/test_gpu_adjoint.py: <= 1e-3 relative vs the FP64 implicit adjoint",
+        "roofline": {
+            "bound": "latency: 2,673 vertices give under 1% of the GPU's resident threads work",
+            "achieved": alg / tb / 1e9,
+            "peak": peak,
+            "peak_source": peak_kind,
+            "unit": "GB/s",
+            "frac": alg / tb / 1e9 / peak,
+            "alg_bytes_backward": alg,
+            "how": "algorithmic bytes of the backward (recomputed forward sweeps + adjoint sweeps) over its wall "
+                   "time around the C-ABI call (uploads and read-backs included)",
+        },
     }
 
 
@@ -455,7 +560,7 @@ def bench_material_id(local, stream):
     """Batched material identification: 64 beams (Lx U{8..40}, Ly = Lz U{3..8}), hidden (E, nu) as the
     batched configuration, targets from a 20-step forward under gravity; per-mesh gradients of
     (log E, nu) from one batched forward + adjoint vs central finite differences of the batched
-    forward (step 1e-3) at the initial guess, then 50 Adam iterations from E = 1e5, nu = 0.3."""
+    forward (step 1e-3) at the initial guess, then 50 per-mesh quasi-Newton iterations from E = 1e5, nu = 0.3."""
     import torch
 
     from vbd_tetmesh_b200 import material_id as mid
@@ -472,7 +577,7 @@ def bench_material_id(local, stream):
         fE = prob.fd_grad(logE0, nu0, targets, "logE", 1e-3)
         fN = prob.fd_grad(logE0, nu0, targets, "nu", 1e-3)
         t0 = time.perf_counter()
-        logE, nu, hist = mid.identify(prob, targets, logE0, nu0, outer=50)
+        logE, nu, hist, final_losses = mid.identify(prob, targets, logE0, nu0, outer=50)
         t_id = time.perf_counter() - t0
         prob.solver.close()
     eE = np.abs(gE - fE) / np.maximum(np.abs(fE), 1e-30)
@@ -488,10 +593,15 @@ def bench_material_id(local, stream):
         "gradient_seconds": t_grad,
         "grad_vs_fd_rel_logE": q(eE),
         "grad_vs_fd_rel_nu": q(eN),
+        "grad_fd": "central differences of the batched FP32 GPU forward, step 1e-3 (FP32 noise dominates at 1e-4); "
+                   "checked against FP64 finite differences at converged iterations in tests/test_gpu_material_id.py",
+        "optimizer": "per-mesh quasi-Newton (2x2 BFGS on log E, nu/0.1) with per-mesh backtracking line search; "
+                     "every trial is one batched forward + adjoint of all meshes",
         "outer_iterations": 50,
         "identify_seconds": t_id,
         "loss_first": hist[0],
         "loss_last": hist[-1],
+        "final_loss_per_mesh": q(np.asarray(final_losses)),
         "recovered_E_rel_err": q(relE),
         "recovered_nu_abs_err": q(dnu),
     }
@@ -687,7 +797,9 @@ def main():
             "unit": UNIT,
             "cores": cores,
             "kind": kind,
-            "sample": f"3 samples of 1 cube iteration (274,625 vertices, after 1 warm-up): {what}",
+            "sample": f"3 samples of 1 cube iteration (274,625 vertices, after 1 warm-up): {what}; its colour loop "
+                      "runs one colour per thread, so at most 8 threads (the cube's 8 colours) are busy",
+            "restatement": cpu_restatement(mesh),
         }
     solver.close()
     if rank == 0:

@@ -7,6 +7,9 @@
 #include <cmath>
 #include <cstdint>
 #include <functional>
+#ifdef VBD_DEBUG
+#include <iostream>
+#endif
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -52,6 +55,15 @@ using TTetVIdsArr = TetVIdsArr;
 
 #ifndef EPSILON
 #define EPSILON 1e-8
+#endif
+
+// Debug output, as the reference's Types.h:72-77: printed in VBD_DEBUG builds only.
+#ifndef VBD_LOG
+#ifdef VBD_DEBUG
+#define VBD_LOG(msg) std::cout << "[VBD] " << msg << std::endl
+#else
+#define VBD_LOG(msg)
+#endif
 #endif
 
 // Throws std::runtime_error with vbd_last_error() when a C-ABI call fails.

@@ -5,11 +5,13 @@
 // execute through libvbd_b200: the TetMesh's positions and velocities are uploaded, one
 // vbd_solver_step runs on the device, and positions, velocities and the inertial target are read
 // back.  Colouring and Dm^-1 / V0 are computed by the library bit-exactly with the reference.
+// energyHistory is filled as the reference fills it: computeTotalEnergy after iterations 0, 10,
+// 20, ... of every sub-step (VBD.cpp:93-95), evaluated on the device inside the step (FP64 sums)
+// and read back once per step; simulate() clears it first and evaluates the energy once more after
+// every frame, which the reference only prints in VBD_DEBUG builds (VBD.cpp:313-330).
 // Differences from the reference, by design:
 //   * numThreads is ignored (the GPU sweeps each colour in parallel; results equal the reference's
 //     single-thread run up to summation order, without its colour-loop race, VBD.cpp:120);
-//   * energyHistory gets one computeTotalEnergy value per step when recordEnergyHistory is set
-//     (the reference evaluates it every 10th iteration inside step);
 //   * solveVertex / computeTetContribution (per-vertex CPU helpers) are not provided.
 #pragma once
 
@@ -35,7 +37,6 @@ struct VBDParams {
     Real density = 1000.0f;
     // extensions
     bool usePerTetMaterials = false;   // use TetMesh::tetMu / tetLambda instead of mu / lambda
-    bool recordEnergyHistory = false;  // push computeTotalEnergy after every step
     int device = 0;                    // CUDA device of the solver
 };
 
@@ -83,13 +84,22 @@ class VBDsolver {
         vbdCheck(vbd_solver_get_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_get_positions");
         vbdCheck(vbd_solver_get_velocities(gpu_, mesh.mVelocity.data()), "vbd_solver_get_velocities");
         vbdCheck(vbd_solver_get_inertia(gpu_, mesh.mInertia.data()), "vbd_solver_get_inertia");
-        if (params.recordEnergyHistory) energyHistory.push_back(computeTotalEnergy(mesh));
+        // the energies the step evaluated after iterations 0, 10, 20, ... (VBD.cpp:93-95)
+        int32_t n = 0;
+        vbdCheck(vbd_solver_energy_history(gpu_, nullptr, 0, &n, 0), "vbd_solver_energy_history");
+        std::vector<double> e((size_t)n);
+        vbdCheck(vbd_solver_energy_history(gpu_, e.data(), n, &n, 1), "vbd_solver_energy_history");
+        for (double v : e) energyHistory.push_back((Real)v);
     }
 
     void simulate(TetMesh& mesh, int numFrames, std::function<void(int, TetMesh&)> callback = nullptr) {
         energyHistory.clear();
         for (int frame = 0; frame < numFrames; ++frame) {
             step(mesh);
+            // the frame's energy (VBD.cpp:318-319), from the state the step left on the device
+            const Real energy = deviceEnergy();
+            VBD_LOG("Frame " << frame << " completed, Energy: " << energy);
+            (void)energy;
             if (callback) callback(frame, mesh);
         }
     }
@@ -99,9 +109,7 @@ class VBDsolver {
     Real computeTotalEnergy(const TetMesh& mesh) const {
         ensureDevice(mesh);
         vbdCheck(vbd_solver_set_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_set_positions");
-        double e = 0.0;
-        vbdCheck(vbd_solver_energy(gpu_, VBD_ENERGY_ELASTIC_LOGJ, 1.0f, &e), "vbd_solver_energy");
-        return (Real)e;
+        return deviceEnergy();
     }
 
     const std::vector<std::vector<IdType>>& getVertexColors() const { return vertexColors; }
@@ -167,12 +175,23 @@ class VBDsolver {
         return flat;
     }
 
+    // computeTotalEnergy of the positions on the device (no upload).
+    Real deviceEnergy() const {
+        double e = 0.0;
+        vbdCheck(vbd_solver_energy(gpu_, VBD_ENERGY_ELASTIC_LOGJ, 1.0f, &e), "vbd_solver_energy");
+        return (Real)e;
+    }
+
     void ensureDevice(const TetMesh& mesh) const {
         if (gpu_ && devVerts_ == mesh.numVerts && devTets_ == mesh.numTets) {
             syncMaterials(mesh);
             return;
         }
-        if (!gpu_) vbdCheck(vbd_solver_create(&gpu_, params.device, nullptr), "vbd_solver_create");
+        if (!gpu_) {
+            vbdCheck(vbd_solver_create(&gpu_, params.device, nullptr), "vbd_solver_create");
+            // VBDsolver::step evaluates computeTotalEnergy every 10th iteration (VBD.cpp:93-95)
+            vbdCheck(vbd_solver_set_option(gpu_, VBD_OPT_ENERGY_EVERY, 10), "vbd_solver_set_option");
+        }
         const std::vector<int32_t> flat = flatTets(mesh);
         std::vector<uint8_t> fixed(mesh.numVerts);
         for (size_t i = 0; i < mesh.numVerts; ++i) fixed[i] = mesh.isFixed[i] ? 1 : 0;

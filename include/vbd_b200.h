@@ -216,6 +216,12 @@ int vbd_solver_sync(vbd_solver* s);
  * after spin_limit polls and exits; *timed_out receives 1 if the device recorded the timeout. */
 int vbd_solver_barrier_selftest(vbd_solver* s, int64_t spin_limit, int32_t* timed_out);
 
+/* The energy history of VBD_OPT_ENERGY_EVERY (VBDsolver::energyHistory, VBD.h:70; filled at
+ * VBD.cpp:93-95): writes up to `capacity` values, oldest first, and sets *count to the number of
+ * values appended since the last reset (a count above capacity means the rest were not copied).
+ * reset != 0 empties the history.  Completes the queued work first. */
+int vbd_solver_energy_history(vbd_solver* s, double* energies, int32_t capacity, int32_t* count, int32_t reset);
+
 /* Energies (FP64 accumulation over the FP32 state).  Completes before returning.
  *   VBD_ENERGY_IP:      incremental potential sum_i m_i/(2h^2)|x_i - y_i|^2 + sum_t V_t psi(F_t),
  *                       psi = mu/2(|F|^2-3) - mu(J-1) + lambda/2 (J-1)^2 (the energy whose gradient
@@ -260,9 +266,10 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *                        event pair on the handle's stream (read with vbd_solver_kernel_time)
  *   VBD_OPT_PREFETCH:    0 = load each element record where it is used, 1 = load the next record
  *                        while evaluating the current one, 2 = load a lane's first three records
- *                        before the sweep's dependency wait (layouts 3 and 4; others run 1).  Until
- *                        it is set: 2 with layout 4 when no lane holds more than three records
- *                        (most incident tets of a free vertex / lanes), else 1.  All give the same bits
+ *                        before the sweep's dependency wait, 3 = its first two, in a kernel held to
+ *                        56 registers (2 and 3: layouts 3 and 4; others run 1).  Until it is set: 2
+ *                        with layout 4 when no lane holds more than three records (most incident
+ *                        tets of a free vertex / lanes), else 1.  All give the same bits
  *   VBD_OPT_PDL:         1 = launch colour sweeps with programmatic dependent launch, so a sweep
  *                        loads its element data while the previous sweep drains
  *   VBD_OPT_BLOCK:       threads per block of the sweep kernel: 64, 128 or 256
@@ -284,7 +291,19 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *                        energies and residuals stay the Neo-Hookean ones
  *   VBD_OPT_L2_PREFETCH: 1 = with the compact or factored layout, each colour sweep prefetches the
  *                        records of the colour swept next into L2 (one bulk prefetch per block);
- *                        off by default (slower on the measured meshes) */
+ *                        off by default (slower on the measured meshes)
+ *   VBD_OPT_RECORD_CACHE: 1 = the factored records (layouts 3 and 4) are loaded past L1 with an L2
+ *                        evict-first policy, so that the stream does not push the vertex state out of
+ *                        L2; same results
+ *   VBD_OPT_RECORD_PERSIST_MB: with VBD_OPT_RECORD_CACHE, the first this-many megabytes of the record
+ *                        stream are loaded with an L2 evict-last policy instead, so that they stay in
+ *                        L2 from one sweep to the next (0 = none)
+ *   VBD_OPT_ENERGY_EVERY: k > 0 = vbd_solver_step also evaluates VBDsolver::computeTotalEnergy (the
+ *                        VBD_ENERGY_ELASTIC_LOGJ energy, FP64 sums) of the positions after iterations
+ *                        0, k, 2k, ... of every sub-step, as VBDsolver::step does with k = 10
+ *                        (VBD.cpp:93-95), into a device-side history read by
+ *                        vbd_solver_energy_history; 0 = off (the default).  Positions are unchanged.
+ *                        With VBD_OPT_PERSISTENT the steps then run as separate launches */
 typedef enum vbd_option {
     VBD_OPT_LANES = 0,
     VBD_OPT_LAYOUT = 1,
@@ -296,16 +315,35 @@ typedef enum vbd_option {
     VBD_OPT_PERSISTENT = 7,
     VBD_OPT_ADJOINT_ALTERNATE = 8,
     VBD_OPT_SEMANTICS = 9,
-    VBD_OPT_L2_PREFETCH = 10
+    VBD_OPT_L2_PREFETCH = 10,
+    VBD_OPT_RECORD_CACHE = 11,
+    VBD_OPT_RECORD_PERSIST_MB = 12,
+    VBD_OPT_ENERGY_EVERY = 13
 } vbd_option;
 int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value);
 int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value);
 
+/* Per-colour launch shape (no reference counterpart; the reference's kernel runs 16 threads per
+ * vertex for every colour, VBD_GPU_Wrapper.cu:349): colour c of the sweep runs lanes[c] threads per
+ * vertex (1, 2, 4, 8, 16 or 32), and its record prefetch follows the lane count as VBD_OPT_PREFETCH
+ * describes.  lanes = NULL goes back to VBD_OPT_LANES for every colour.  Same results as the
+ * uniform shape up to the order of the per-vertex sums.  A new mesh (vbd_solver_init) clears it.
+ * get_colour_lanes writes the lane count each colour runs. */
+int vbd_solver_set_colour_lanes(vbd_solver* s, int32_t num_colours, const int32_t* lanes);
+int vbd_solver_get_colour_lanes(vbd_solver* s, int32_t num_colours, int32_t* lanes);
+
 /* Autotuner: times `repeats` steps of `iterations` sweeps (dt, no gravity, Chebyshev 0.9) for each
- * launch shape in a fixed candidate list -- threads per vertex, record layout, prefetch, programmatic
- * dependent launch, block size -- keeps the fastest, and restores the simulation state (positions,
- * velocities, inertia, counters) it started from.  chosen (may be null) receives 5 ints:
- * lanes, layout, prefetch, pdl, block. */
+ * launch configuration it tries and keeps the fastest, then restores the simulation state
+ * (positions, velocities, inertia, counters) it started from.  In order:
+ *   1. uniform launch shapes from a fixed list -- threads per vertex, record layout, prefetch,
+ *      programmatic dependent launch, block size;
+ *   2. the factored records' L2 policy (VBD_OPT_RECORD_CACHE);
+ *   3. per-colour threads per vertex, colour by colour, half and double the current count
+ *      (vbd_solver_set_colour_lanes);
+ *   4. the persistent colour-walking kernel (VBD_OPT_PERSISTENT) against the captured graph.
+ * Phases 2-4 replace the choice only when faster by more than 1%.  chosen (may be null) receives 5
+ * ints: lanes, layout, prefetch, pdl, block; the rest of the choice is read back with
+ * vbd_solver_get_option (VBD_OPT_RECORD_CACHE, VBD_OPT_PERSISTENT) and vbd_solver_get_colour_lanes. */
 int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t repeats, int32_t* chosen);
 
 /* Allocation-free incremental potential.  No counterpart in the reference: it exists for callers
@@ -319,9 +357,11 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
  * error flag) is a fixed 32 KiB __device__ array that every GPU loading the library holds until
  * exit, so num_verts + num_tets is limited to 16,777,216 (larger sizes return
  * VBD_ERR_INVALID_ARG).  The first call on each device looks up the scratch address and must come
- * before any stream capture on that device.  Calls share the scratch: calls that overlap on the
- * GPU race.  Runs on `cuda_stream` (null = default stream) and completes before returning; tets
- * with ids outside [0, N) are skipped and reported as VBD_ERR_INVALID_ARG. */
+ * before any stream capture on that device; later calls look it up again unless their stream is
+ * capturing, so a cudaDeviceReset between calls is harmless.  Calls share the scratch: calls that
+ * overlap on the GPU race.  Runs on `cuda_stream` (null = default stream) and blocks the calling
+ * thread until it completes; tets with ids outside [0, N) are skipped and reported as
+ * VBD_ERR_INVALID_ARG. */
 int vbd_ip_energy_noalloc(int32_t num_verts, int32_t num_tets, const float* positions, const float* inertia,
                           const float* vertex_mass, const int32_t* tets, const float* dm_inv, const float* rest_vol,
                           const float* tet_mu, const float* tet_lambda, float h, double* out, void* cuda_stream);

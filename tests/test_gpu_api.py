@@ -3,7 +3,7 @@ status counters, options and host-made fault cases (none of which faults the GPU
 import numpy as np
 import pytest
 
-from helpers import rel_err, small_block
+from helpers import gpu_simulate, rel_err, small_block
 from oracle import pyoracle as po
 from vbd_tetmesh_b200 import GPUSolver, VBDError, build_solver, color_vertices, mesh_mass, meshgen, precompute_tets
 from vbd_tetmesh_b200 import _capi
@@ -248,6 +248,9 @@ def test_autotune_restores_state_and_keeps_parity(gpu_device):
     v0 = s.get_velocities()
     chosen = s.autotune(1 / 120, iterations=5, repeats=1)
     assert chosen["lanes"] in (2, 4, 8, 16) and chosen["layout"] in (0, 1, 2, 3, 4)
+    assert chosen["persistent"] in (0, 1) and chosen["record_cache"] in (0, 1)
+    assert len(chosen["colour_lanes"]) == len(s.colour_groups[0]) - 1
+    assert all(L in (1, 2, 4, 8, 16, 32) for L in chosen["colour_lanes"])
     np.testing.assert_array_equal(s.get_positions(), x0)
     np.testing.assert_array_equal(s.get_velocities(), v0)
     assert s.status() == (0, False)
@@ -255,6 +258,117 @@ def test_autotune_restores_state_and_keeps_parity(gpu_device):
     s.step(st["dt"], 10, st["gravity"], True, st["rho"])
     o = po.simulate(m, 1, st["dt"], 10, st["gravity"], True, st["rho"], precision=32, mode=po.CLOSED)
     assert rel_err(s.get_positions(), o["x"], m) < 1e-5
+
+
+def _step_ms(s, steps, dt, iters):
+    import torch
+
+    s.step(dt, iters, (0.0, 0.0, 0.0), True, 0.9)
+    s.sync()
+    t = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s.step(dt, iters, (0.0, 0.0, 0.0), True, 0.9)
+        s.sync()
+        e1.record()
+        e1.synchronize()
+        t.append(e0.elapsed_time(e1))
+    return float(np.median(t))
+
+
+def test_autotune_chooses_between_graph_and_persistent_by_time(gpu_device):
+    """The autotuner's last phase times the whole step as one persistent colour-walking launch
+    against the captured graph of separate launches and keeps the faster: re-timed afterwards, the
+    path it kept is not slower than the other one beyond timing noise, and both give the same bits."""
+    m = meshgen.cube(16)
+    s = build_solver(m)
+    chosen = s.autotune(1 / 120, iterations=10, repeats=3)
+    kept = chosen["persistent"]
+    t_kept = _step_ms(s, 5, 1 / 120, 10)
+    xa = s.get_positions()
+    s.set_option(_capi.OPT_PERSISTENT, 1 - kept)
+    s.set_colour_lanes(None)
+    t_other = _step_ms(s, 5, 1 / 120, 10)
+    print(f"autotune kept persistent={kept}: {t_kept:.3f} ms/step; the other path {t_other:.3f} ms/step; {chosen}")
+    assert t_kept <= 1.25 * t_other
+    s.close()
+    assert np.all(np.isfinite(xa))
+
+
+@pytest.mark.parametrize("lanes", [[4, 8, 16, 8, 4, 16, 8, 2], [16] * 8])
+def test_per_colour_lanes_match_oracle(gpu_device, lanes):
+    """Per-colour threads per vertex (vbd_solver_set_colour_lanes): within the parity bar of the
+    oracle; a uniform per-colour setting equals the uniform option bit for bit."""
+    m = meshgen.cube(10)
+    st = meshgen.CUBE_SETTINGS
+    s = build_solver(m)
+    nc = len(s.get_colour_lanes())
+    cl = (lanes * nc)[:nc]
+    s.set_colour_lanes(cl)
+    assert s.get_colour_lanes().tolist() == cl
+    for _ in range(3):
+        s.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])
+    x = s.get_positions()
+    s.close()
+    o = po.simulate(m, 3, st["dt"], st["iterations"], st["gravity"], True, st["rho"], precision=32, mode=po.CLOSED)
+    assert rel_err(x, o["x"], m) < 1e-5
+    if len(set(cl)) == 1:
+        u = gpu_simulate(m, 3, st["dt"], st["iterations"], st["gravity"], True, st["rho"], lanes=cl[0])
+        np.testing.assert_array_equal(x, u["x"])
+
+
+def test_colour_lanes_validation(gpu_device):
+    m = small_block(seed=3)
+    s = build_solver(m)
+    nc = len(s.get_colour_lanes())
+    with pytest.raises(VBDError):
+        s.set_colour_lanes([8] * (nc + 1))
+    with pytest.raises(VBDError):
+        s.set_colour_lanes([3] * nc)
+    s.set_colour_lanes([4] * nc)
+    s.set_colour_lanes(None)
+    assert s.get_colour_lanes().tolist() == [s.get_option(_capi.OPT_LANES)] * nc
+    s.close()
+
+
+@pytest.mark.parametrize("layout", [3, 4])
+def test_record_cache_and_two_deep_prefetch_change_no_bits(gpu_device, layout):
+    """The L2 policy of the record loads (evict-first, with an evict-last prefix) and the two-deep
+    prefetch held to 56 registers change no arithmetic: bit-identical positions."""
+    m = meshgen.cube(12)
+    st = meshgen.CUBE_SETTINGS
+    base = gpu_simulate(m, 2, st["dt"], st["iterations"], st["gravity"], True, st["rho"], layout=layout)
+    for opts in ({_capi.OPT_RECORD_CACHE: 1}, {_capi.OPT_RECORD_CACHE: 1, _capi.OPT_RECORD_PERSIST_MB: 1},
+                 {_capi.OPT_PREFETCH: 3}, {_capi.OPT_PREFETCH: 3, _capi.OPT_RECORD_CACHE: 1}):
+        g = gpu_simulate(m, 2, st["dt"], st["iterations"], st["gravity"], True, st["rho"], layout=layout,
+                         options=opts)
+        np.testing.assert_array_equal(g["x"], base["x"])
+        np.testing.assert_array_equal(g["v"], base["v"])
+
+
+def test_energy_history_matches_oracle(gpu_device):
+    """VBD_OPT_ENERGY_EVERY 10: vbd_solver_step appends computeTotalEnergy after iterations 0, 10, 20,
+    ... of every sub-step (VBD.cpp:93-95); equal to the oracle's history within 1e-4 relative, the
+    positions unchanged by it."""
+    m = small_block(seed=13, dims=(7, 4, 4), per_tet_sigma=0.0)
+    dt, iters, substeps, steps = 1 / 60, 25, 2, 3
+    s = build_solver(m)
+    s.set_option(_capi.OPT_ENERGY_EVERY, 10)
+    for _ in range(steps):
+        s.step(dt, iters, (0.0, -9.8, 0.0), True, 0.9, substeps)
+    eh = s.energy_history(reset=False)
+    assert len(eh) == steps * substeps * 3
+    again = s.energy_history(reset=True)
+    np.testing.assert_array_equal(eh, again)
+    assert len(s.energy_history()) == 0
+    x = s.get_positions()
+    s.close()
+    o = po.simulate(m, steps, dt, iters, (0.0, -9.8, 0.0), True, 0.9, substeps=substeps, precision=32,
+                    energy_history=True)
+    np.testing.assert_allclose(eh, o["ehist"][: len(eh)], rtol=1e-4, atol=1e-4 * np.abs(o["ehist"]).max())
+    plain = gpu_simulate(m, steps, dt, iters, (0.0, -9.8, 0.0), True, 0.9, substeps=substeps)
+    np.testing.assert_array_equal(x, plain["x"])
 
 
 def test_layout_switches_rebuild_captured_graphs(gpu_device):

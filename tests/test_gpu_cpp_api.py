@@ -1,6 +1,7 @@
 """The C++ drop-in surface on the GPU: tests/cpp/test_cpp_api runs the reference's two calling
 patterns (VBDsolver::step, and the main.cpp loop over VBD_GPU_Solver) through include/vbd/*.h and
 libvbd_b200; results are checked against the oracle."""
+import importlib.util
 import os
 import subprocess
 
@@ -16,6 +17,8 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CPP_DIR = os.path.join(ROOT, "tests", "cpp")
 BIN = os.path.join(CPP_DIR, "test_cpp_api")
+SIM_BIN = os.path.join(CPP_DIR, "test_simulate")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def run_cpp(m, iters, steps, dt, rho, tmp_path):
@@ -84,3 +87,57 @@ def test_cpp_surface_matches_oracle(gpu_device, tmp_path):
     mu, lam = float(m.mu[0]), float(m.lam[0])
     e = np.sum(v0 * (0.5 * mu * (np.einsum("tij,tij->t", F, F) - 3) - mu * np.log(J) + 0.5 * lam * np.log(J) ** 2))
     assert abs(out["energy"] - e) <= 1e-4 * abs(e)
+
+
+def _ref_cases():
+    """The cases of the reference fixtures (tests/golden/make_ref_golden.py's table)."""
+    spec = importlib.util.spec_from_file_location("make_ref_golden", os.path.join(GOLDEN, "make_ref_golden.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.CASES
+
+
+def run_simulate(m, iters, frames, substeps, accel, dt, rho, tmp_path):
+    if not os.path.exists(SIM_BIN):
+        subprocess.run(["make", "-C", CPP_DIR], check=True, capture_output=True)
+    inp = tmp_path / "sim_in.bin"
+    with open(inp, "wb") as f:
+        np.array([m.num_verts, m.num_tets, iters, frames, substeps, int(accel)], np.int32).tofile(f)
+        np.array([m.density, m.mu[0], m.lam[0], dt, rho], np.float32).tofile(f)
+        for a in (m.rest, m.x, m.v):
+            a.astype(np.float32).tofile(f)
+        m.tets.astype(np.int32).tofile(f)
+        m.fixed.astype(np.uint8).tofile(f)
+    out = tmp_path / "sim_out.bin"
+    r = subprocess.run([SIM_BIN, str(inp), str(out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    raw = open(out, "rb").read()
+    n3 = 3 * m.num_verts
+    f = np.frombuffer(raw[: 8 * n3], np.float32)
+    ints = np.frombuffer(raw[8 * n3: 8 * n3 + 16], np.int32)
+    hist = np.frombuffer(raw[8 * n3 + 16:], np.float32)
+    assert len(hist) == ints[3]
+    return dict(x=f[:n3].reshape(-1, 3), v=f[n3:].reshape(-1, 3), callbacks=int(ints[0]), in_order=bool(ints[1]),
+                positions_match=bool(ints[2]), ehist=hist.astype(np.float64))
+
+
+@pytest.mark.parametrize("case", ["beam", "block_accel_off_sub2", "cube6_stiff"])
+def test_simulate_matches_reference_fixtures(gpu_device, case, tmp_path):
+    """VBDsolver::simulate through the C++ drop-in with a per-frame callback, against the reference's
+    own VBDsolver (fixtures tests/golden/ref_trajectories.npz): positions after 10 frames within 1e-5
+    of the diagonal, and energyHistory -- computeTotalEnergy after iterations 0, 10, 20, ... of every
+    sub-step, VBD.cpp:93-95 -- of the same length and within 1e-4 relative (the reference evaluates it
+    in FP32 through an SVD, this library in FP64 sums)."""
+    make, dt, iters, accel, rho, sub = _ref_cases()[case]
+    m = make()
+    frames = 10
+    out = run_simulate(m, iters, frames, sub, accel, dt, rho, tmp_path)
+    g = np.load(os.path.join(GOLDEN, "ref_trajectories.npz"))
+    assert out["callbacks"] == frames and out["in_order"] and out["positions_match"]
+    err = rel_err(out["x"], g[f"{case}/x_s10"], m)
+    eh = g[f"{case}/ehist"]
+    print(f"simulate {case}: |x - reference|/diag {err:.3e}; energyHistory {len(out['ehist'])} values, max rel "
+          f"{np.max(np.abs(out['ehist'] - eh) / np.abs(eh).max()):.2e}")
+    assert err < 1e-5
+    assert len(out["ehist"]) == len(eh) == frames * sub * ((iters + 9) // 10)
+    np.testing.assert_allclose(out["ehist"], eh, rtol=1e-4, atol=1e-4 * np.abs(eh).max())

@@ -1,0 +1,122 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle on the configurations the throughput
+claims are quoted on, at their own sizes:
+
+* the 64^3 jittered cube (274,625 vertices, 1,572,864 tets; E = 1e6, nu = 0.4, dt = 1/120,
+  50 iterations, Chebyshev 0.9) after 1 and 10 steps, against the FP32 and FP64 oracles;
+* the 512-mesh batch (dims U{4..24}^3) stepped as one batch for 60 steps of 20 iterations, a seeded
+  sample of 16 meshes against the FP64 oracle run of each mesh on its own;
+* the differentiated 32x8x8 beam's forward (per-tet log-normal mu / lambda, 30 iterations) after 1
+  and 10 steps.
+
+Bar (floating point): positions within 1e-5 of the mesh's bounding-box diagonal; the incremental
+potential within 1e-5 relative of the FP32 oracle, or within the distance of the FP32 oracle itself
+from FP64 where that is larger (the FP32 noise floor, printed beside each result).  The oracle runs
+on all host cores (OpenMP within each colour, the same result as one thread).
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_err
+from oracle import pyoracle as po
+from vbd_tetmesh_b200 import build_batch_solver, build_solver, meshgen
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL = 1e-5  # of the bounding-box diagonal
+IP_TOL = 1e-5   # relative
+
+
+def _oracle(m, steps, st, precision, x0=None, v0=None):
+    return po.simulate(m, steps, st["dt"], st["iterations"], st["gravity"], True, st["rho"], precision=precision,
+                       mode=po.CLOSED, threads=po.max_threads(), x0=x0, v0=v0)
+
+
+def _ip_ok(ip_gpu, ip32, ip64):
+    """|gpu - oracle32| within 1e-5 relative, or within |oracle32 - oracle64| (the noise floor)."""
+    return abs(ip_gpu - ip32) <= max(IP_TOL * abs(ip32), abs(ip32 - ip64))
+
+
+def _check_chain(name, m, st, solver):
+    """Steps the solver and the FP32 / FP64 oracles 1 and then 9 more steps (the oracle chained
+    through its own state, which equals a direct 10-step run) and checks both checkpoints."""
+    o32 = o64 = None
+    done = 0
+    for steps in (1, 10):
+        for _ in range(steps - done):
+            solver.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])
+        solver.sync()
+        x = solver.get_positions()
+        ip = solver.energy(0, st["dt"])
+        o32 = _oracle(m, steps - done, st, 32, None if o32 is None else o32["x"], None if o32 is None else o32["v"])
+        o64 = _oracle(m, steps - done, st, 64, None if o64 is None else o64["x"], None if o64 is None else o64["v"])
+        done = steps
+        e32, e64, n64 = rel_err(x, o32["x"], m), rel_err(x, o64["x"], m), rel_err(o32["x"], o64["x"], m)
+        ip32, ip64 = o32["ip"][-1], o64["ip"][-1]
+        print(f"{name} {steps} steps: |gpu - oracle32|/diag {e32:.3e}, |gpu - oracle64|/diag {e64:.3e} "
+              f"(oracle32 vs 64: {n64:.3e}); IP gpu {ip:.9g} vs32 {abs(ip - ip32) / abs(ip32):.2e} "
+              f"vs64 {abs(ip - ip64) / abs(ip64):.2e} (oracle32 vs64 {abs(ip32 - ip64) / abs(ip64):.2e})")
+        assert e32 < POS_TOL
+        assert e64 < POS_TOL
+        assert _ip_ok(ip, ip32, ip64)
+    sing, nonf = solver.status()
+    assert sing == 0 and not nonf
+
+
+def test_cube64_matches_oracle(gpu_device):
+    """The benched workload itself, with the bench's launch shape (chosen at init: packed factored
+    records, 8 lanes, deep record prefetch)."""
+    m = meshgen.cube(64)
+    assert (m.num_verts, m.num_tets) == (274625, 1572864)
+    st = meshgen.CUBE_SETTINGS
+    s = build_solver(m, device=gpu_device)
+    try:
+        _check_chain("cube64", m, st, s)
+    finally:
+        s.close()
+
+
+def test_diff_beam_forward_matches_oracle(gpu_device):
+    m, _, _ = meshgen.diff_beam()
+    st = meshgen.DIFF_SETTINGS
+    s = build_solver(m, device=gpu_device)
+    try:
+        _check_chain("diff_beam", m, st, s)
+    finally:
+        s.close()
+
+
+# The batched configuration's stated sizes; the sample is seeded.
+C4_MESHES, C4_STEPS, C4_SAMPLE, C4_SEED = 512, 60, 16, 77
+C4_SETTINGS = dict(dt=1.0 / 60.0, iterations=20, rho=0.9, gravity=(0.0, -9.8, 0.0))
+
+
+def test_batched_512_sample_matches_fp64(gpu_device):
+    """All 512 meshes advance in one solver (one launch per colour); every sampled mesh's positions
+    after 60 steps lie within 1e-5 of its diagonal of its own FP64 oracle run, and of the FP32 one."""
+    meshes = meshgen.batched_blocks(C4_MESHES)
+    b = meshgen.concat(meshes)
+    st = C4_SETTINGS
+    s = build_batch_solver(b, device=gpu_device)
+    try:
+        for _ in range(C4_STEPS):
+            s.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])
+        s.sync()
+        x = s.get_positions()
+        sing, nonf = s.status()
+    finally:
+        s.close()
+    assert sing == 0 and not nonf
+    idx = sorted(np.random.default_rng(C4_SEED).choice(C4_MESHES, C4_SAMPLE, replace=False).tolist())
+    worst = 0.0
+    for k in idx:
+        m = meshes[k]
+        xk = x[b.vert_offsets[k]:b.vert_offsets[k + 1]]
+        o64 = _oracle(m, C4_STEPS, st, 64)
+        o32 = _oracle(m, C4_STEPS, st, 32)
+        e64, e32 = rel_err(xk, o64["x"], m), rel_err(xk, o32["x"], m)
+        print(f"batch mesh {k} dims {m.dims}: |gpu - oracle64|/diag {e64:.3e}, |gpu - oracle32|/diag {e32:.3e} "
+              f"(oracle32 vs 64: {rel_err(o32['x'], o64['x'], m):.3e})")
+        worst = max(worst, e64)
+        assert e64 < POS_TOL
+        assert e32 < POS_TOL
+    print(f"batch sample of {len(idx)} meshes after {C4_STEPS} steps: worst |gpu - oracle64|/diag {worst:.3e}")

@@ -39,6 +39,9 @@ OPT_PERSISTENT = 7
 OPT_ADJOINT_ALTERNATE = 8
 OPT_SEMANTICS = 9
 OPT_L2_PREFETCH = 10
+OPT_RECORD_CACHE = 11
+OPT_RECORD_PERSIST_MB = 12
+OPT_ENERGY_EVERY = 13
 SEMANTICS_VBDSOLVER = 0
 SEMANTICS_GPU_WRAPPER = 1
 
@@ -78,10 +81,13 @@ SIGNATURES = {
     "vbd_solver_record": [_p, _i32],
     "vbd_solver_backward": [_p, _p, _p, _i32, _f32, _p, _p, _p, _p],
     "vbd_solver_energy": [_p, _i32, _f32, _PF64],
+    "vbd_solver_energy_history": [_p, _p, _i32, _PI32, _i32],
     "vbd_solver_status": [_p, _PI64, _PI32, _i32],
     "vbd_solver_set_option": [_p, _i32, _i32],
     "vbd_solver_get_option": [_p, _i32, _PI32],
     "vbd_solver_info": [_p, _PI32, _PI32, _PI32],
+    "vbd_solver_set_colour_lanes": [_p, _i32, _p],
+    "vbd_solver_get_colour_lanes": [_p, _i32, _p],
     "vbd_solver_kernel_launches": [_p, _PI64],
     "vbd_solver_kernel_time": [_p, _PF64, _PI64, _PF64, _i32],
     "vbd_solver_autotune": [_p, _f32, _i32, _i32, _p],

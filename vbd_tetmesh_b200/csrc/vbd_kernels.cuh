@@ -48,10 +48,13 @@ struct SweepParams {
     float omega;
     int accel;                 // write x^(k) = omega (x~ - pp) + pp to xnext (VBD.cpp:290-300)
     int keep_pp;               // store the pre-sweep position into pp (VBD.cpp:78,89)
-    // Unused by the kernels.  It keeps this block above 128 bytes: on the 64^3 cube the step
-    // measured 4.61 ms at 136 bytes (and the same at 152 to 264), 4.81 ms at 128 and 5.05 ms at
-    // 120 (A/B on one B200, kernel arithmetic unchanged); the cause is not known.
-    const void* reserved;
+    // Streamed records of incidences below persist_end are read with the L2 evict-last policy, the
+    // rest evict-first (kernels built with a record cache policy only).  The two ints also keep
+    // this block above 128 bytes: on the 64^3 cube the step measured 4.61 ms at 136 bytes (and the
+    // same at 152 to 264), 4.81 ms at 128 and 5.05 ms at 120 (A/B on one B200, kernel arithmetic
+    // unchanged); the cause is not known.
+    int persist_end;
+    int reserved_;
     const char* l2_next;       // element records of the colour swept next (16 B aligned), prefetched
     unsigned long long l2_bytes;  // into L2 while this colour runs; 0 = none
 };
@@ -356,6 +359,59 @@ __device__ __forceinline__ FactRaw4 load_fact_packed(const int4* __restrict__ cr
     return r;
 }
 
+// L2 eviction policy of a streamed record load (createpolicy): evict-first for records that are
+// read once per sweep, so that they do not push the vertex state out of L2; evict-last for the
+// share of the stream that is kept resident across sweeps.
+__device__ __forceinline__ unsigned long long record_policy(bool keep) {
+    unsigned long long first, last;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(first));
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(last));
+    return keep ? last : first;
+}
+
+// Read-only record loads with an L2 policy; the records bypass L1, which keeps its capacity for
+// the neighbour positions.
+__device__ __forceinline__ int4 ld_rec(const int4* p, unsigned long long pol) {
+    int4 r;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
+        : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+        : "l"(p), "l"(pol));
+    return r;
+}
+
+__device__ __forceinline__ float4 ld_rec(const float4* p, unsigned long long pol) {
+    float4 r;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+        : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+        : "l"(p), "l"(pol));
+    return r;
+}
+
+__device__ __forceinline__ float2 ld_rec(const float2* p, unsigned long long pol) {
+    float2 r;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f32 {%0,%1}, [%2], %3;"
+        : "=f"(r.x), "=f"(r.y)
+        : "l"(p), "l"(pol));
+    return r;
+}
+
+__device__ __forceinline__ FactRaw4 load_fact_packed(const int4* __restrict__ crec, const float2* __restrict__ cmat,
+                                                     int j, unsigned long long pol) {
+    FactRaw4 r;
+    r.w0 = ld_rec(crec + 2 * j, pol);
+    r.w1 = ld_rec(reinterpret_cast<const float4*>(crec) + 2 * j + 1, pol);
+    r.m = ld_rec(cmat + j, pol);
+    return r;
+}
+
+__device__ __forceinline__ FactRaw3 load_fact(const int4* __restrict__ crec, int j, unsigned long long pol) {
+    FactRaw3 r;
+    r.w0 = ld_rec(crec + 3 * j, pol);
+    r.w1 = ld_rec(reinterpret_cast<const float4*>(crec) + 3 * j + 1, pol);
+    r.w2 = ld_rec(reinterpret_cast<const float4*>(crec) + 3 * j + 2, pol);
+    return r;
+}
+
 __device__ __forceinline__ FactRec decode_fact(const FactRaw4& w) {
     const unsigned lo = (unsigned)w.w0.x, hi = (unsigned)w.w0.y;
     FactRec r;
@@ -431,11 +487,16 @@ __device__ __forceinline__ void group_reduce(Acc& a) {
 // Element data of incidence j under each record layout:
 //   0 = tet record gathered through inc_tet, 1 = tet record streamed in incidence order,
 //   2 = compact streamed record, 3 = factored streamed record, 4 = packed factored record.
+// fetch_hint loads the factored records with an L2 policy (record_policy); the other layouts
+// ignore the policy.
 template <int LAYOUT> struct Elem;
 template <> struct Elem<0> {
     using Rec = TetRec;
     __device__ __forceinline__ static Rec fetch(const SweepParams& p, int j) {
         return load_rec(p.rec + __ldg(p.inc_tet + j));
+    }
+    __device__ __forceinline__ static Rec fetch_hint(const SweepParams& p, int j, unsigned long long) {
+        return fetch(p, j);
     }
     template <bool COHERENT>
     __device__ __forceinline__ static void contrib(const Rec& r, int v, float4 xi, const float4* X, Acc& acc) {
@@ -445,6 +506,9 @@ template <> struct Elem<0> {
 template <> struct Elem<1> {
     using Rec = TetRec;
     __device__ __forceinline__ static Rec fetch(const SweepParams& p, int j) { return load_rec(p.irec + j); }
+    __device__ __forceinline__ static Rec fetch_hint(const SweepParams& p, int j, unsigned long long) {
+        return fetch(p, j);
+    }
     template <bool COHERENT>
     __device__ __forceinline__ static void contrib(const Rec& r, int v, float4 xi, const float4* X, Acc& acc) {
         tet_contrib<true, COHERENT>(r, v, xi, X, acc);
@@ -453,6 +517,9 @@ template <> struct Elem<1> {
 template <> struct Elem<2> {
     using Rec = CompactRec;
     __device__ __forceinline__ static Rec fetch(const SweepParams& p, int j) { return load_compact(p.crec, p.cmat, j); }
+    __device__ __forceinline__ static Rec fetch_hint(const SweepParams& p, int j, unsigned long long) {
+        return fetch(p, j);
+    }
     template <bool COHERENT>
     __device__ __forceinline__ static void contrib(const Rec& r, int, float4 xi, const float4* X, Acc& acc) {
         compact_contrib<true, COHERENT>(r, xi, X, acc);
@@ -461,6 +528,9 @@ template <> struct Elem<2> {
 template <> struct Elem<3> {
     using Rec = FactRaw3;
     __device__ __forceinline__ static Rec fetch(const SweepParams& p, int j) { return load_fact(p.crec, j); }
+    __device__ __forceinline__ static Rec fetch_hint(const SweepParams& p, int j, unsigned long long pol) {
+        return load_fact(p.crec, j, pol);
+    }
     template <bool COHERENT>
     __device__ __forceinline__ static void contrib(const Rec& r, int, float4 xi, const float4* X, Acc& acc) {
         fact_contrib<true, COHERENT>(decode_fact(r), xi, X, acc);
@@ -471,6 +541,9 @@ template <> struct Elem<4> {
     using Rec = FactRaw4;
     __device__ __forceinline__ static Rec fetch(const SweepParams& p, int j) {
         return load_fact_packed(p.crec, p.cmat, j);
+    }
+    __device__ __forceinline__ static Rec fetch_hint(const SweepParams& p, int j, unsigned long long pol) {
+        return load_fact_packed(p.crec, p.cmat, j, pol);
     }
     template <bool COHERENT>
     __device__ __forceinline__ static void contrib(const Rec& r, int, float4 xi, const float4* X, Acc& acc) {
@@ -491,9 +564,16 @@ template <> struct Elem<4> {
 template <int LANES>
 __device__ __forceinline__ void vertex_solve(const SweepParams& p, int v, int lane, bool active, float4 xi, Acc& acc);
 
-template <int LANES, int LAYOUT, bool PREFETCH, bool COHERENT>
+// Record j of a sweep: plain read-only loads, or (CACHE) loads with the L2 policy `pol`.
+template <int LAYOUT, bool CACHE>
+__device__ __forceinline__ typename Elem<LAYOUT>::Rec fetch_rec(const SweepParams& p, int j, unsigned long long pol) {
+    if constexpr (CACHE) return Elem<LAYOUT>::fetch_hint(p, j, pol);
+    else return Elem<LAYOUT>::fetch(p, j);
+}
+
+template <int LANES, int LAYOUT, bool PREFETCH, bool COHERENT, bool CACHE = false>
 __device__ __forceinline__ void vertex_update(const SweepParams& p, int v, int lane, bool active, int j, int j1,
-                                              typename Elem<LAYOUT>::Rec nxt) {
+                                              typename Elem<LAYOUT>::Rec nxt, unsigned long long pol = 0) {
     const float4 xi = active ? p.x[v] : make_float4(0.f, 0.f, 0.f, 0.f);
     Acc acc;
     acc.zero();
@@ -501,9 +581,9 @@ __device__ __forceinline__ void vertex_update(const SweepParams& p, int v, int l
         typename Elem<LAYOUT>::Rec r;
         if (PREFETCH) {
             r = nxt;
-            if (j + LANES < j1) nxt = Elem<LAYOUT>::fetch(p, j + LANES);
+            if (j + LANES < j1) nxt = fetch_rec<LAYOUT, CACHE>(p, j + LANES, pol);
         } else {
-            r = Elem<LAYOUT>::fetch(p, j);
+            r = fetch_rec<LAYOUT, CACHE>(p, j, pol);
         }
         Elem<LAYOUT>::template contrib<COHERENT>(r, v, xi, p.x, acc);
     }
@@ -583,7 +663,9 @@ __device__ __forceinline__ void l2_prefetch_share(const char* base, unsigned lon
 //            lane with at most k records pays no DRAM round trip after the wait; same summation
 //            order, so the same bits as PREFETCH 1.  (Keeping k records in flight past the first k,
 //            as a ring, took 70-80 registers and ran slower.)
-template <int LANES, int LAYOUT, int PREFETCH>
+//   CACHE:   records loaded with an L2 policy: evict-last for incidences below p.persist_end, else
+//            evict-first (the factored layouts; the others ignore it).  Same bits either way.
+template <int LANES, int LAYOUT, int PREFETCH, bool CACHE = false>
 __device__ __forceinline__ void sweep_body(const SweepParams& p) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = LANES == 1 ? 0 : (threadIdx.x & (LANES - 1));
@@ -595,11 +677,12 @@ __device__ __forceinline__ void sweep_body(const SweepParams& p) {
         j1 = __ldg(p.inc_off + v + 1);
     }
     const int j = j0 + lane;
+    const unsigned long long pol = CACHE ? record_policy(j0 < p.persist_end) : 0ull;
     if constexpr (PREFETCH >= 2) {
         typename Elem<LAYOUT>::Rec buf[PREFETCH];
 #pragma unroll
         for (int k = 0; k < PREFETCH; ++k)
-            if (j + k * LANES < j1) buf[k] = Elem<LAYOUT>::fetch(p, j + k * LANES);
+            if (j + k * LANES < j1) buf[k] = fetch_rec<LAYOUT, CACHE>(p, j + k * LANES, pol);
         if (p.l2_bytes && threadIdx.x == 0) l2_prefetch_share(p.l2_next, p.l2_bytes);
         pdl_trigger();
         pdl_wait();
@@ -610,30 +693,30 @@ __device__ __forceinline__ void sweep_body(const SweepParams& p) {
         for (int k = 0; k < PREFETCH; ++k)
             if (j + k * LANES < j1) Elem<LAYOUT>::template contrib<false>(buf[k], v, xi, p.x, acc);
         for (int jj = j + PREFETCH * LANES; jj < j1; jj += LANES)
-            Elem<LAYOUT>::template contrib<false>(Elem<LAYOUT>::fetch(p, jj), v, xi, p.x, acc);
+            Elem<LAYOUT>::template contrib<false>(fetch_rec<LAYOUT, CACHE>(p, jj, pol), v, xi, p.x, acc);
         vertex_solve<LANES>(p, v, lane, active, xi, acc);
     } else {
         typename Elem<LAYOUT>::Rec nxt;
-        if (PREFETCH && j < j1) nxt = Elem<LAYOUT>::fetch(p, j);
+        if (PREFETCH && j < j1) nxt = fetch_rec<LAYOUT, CACHE>(p, j, pol);
         if (p.l2_bytes && threadIdx.x == 0) l2_prefetch_share(p.l2_next, p.l2_bytes);
         pdl_trigger();
         pdl_wait();
-        vertex_update<LANES, LAYOUT, PREFETCH != 0, false>(p, v, lane, active, j, j1, nxt);
+        vertex_update<LANES, LAYOUT, PREFETCH != 0, false, CACHE>(p, v, lane, active, j, j1, nxt, pol);
     }
 }
 
-template <int LANES, int LAYOUT, int PREFETCH>
+template <int LANES, int LAYOUT, int PREFETCH, bool CACHE = false>
 __global__ void __launch_bounds__(256) k_sweep(SweepParams p) {
-    sweep_body<LANES, LAYOUT, PREFETCH>(p);
+    sweep_body<LANES, LAYOUT, PREFETCH, CACHE>(p);
 }
 
 // The factored layouts with one record ahead, held to 56 registers: they fit without spilling (62-63
 // uncapped), which raises occupancy from 16 to 18 blocks of 64 threads per SM.  Same body, same
 // bits.  Measured on one box: 7.10 against 7.48 ms per step on the 512-mesh batch, 4.48 against 4.58
 // ms on the 64^3 cube.  The deep prefetch spills at 56 and runs slower, so it keeps k_sweep.
-template <int LANES, int LAYOUT>
+template <int LANES, int LAYOUT, int PREFETCH = 1, bool CACHE = false>
 __global__ void __maxnreg__(56) k_sweep_capped(SweepParams p) {
-    sweep_body<LANES, LAYOUT, 1>(p);
+    sweep_body<LANES, LAYOUT, PREFETCH, CACHE>(p);
 }
 
 // ---- VBD_GPU_Solver semantics (the reference's GPU wrapper) ------------------------------------
@@ -990,6 +1073,180 @@ __global__ void __launch_bounds__(256, 4) k_persistent(PersistParams p) {
                 vertex_update<LANES, LAYOUT, true, true>(sp, v, lane, active, j, j1, nxt);
             }
             if (!grid_barrier(p.bar, p.expected_blocks, p.spin_limit, p.sw.status)) return;
+        }
+        if (blend) cur ^= 1;
+    }
+    for (int i = gtid; i < p.nfree; i += nthreads) {
+        const float4 xf = cur ? p.xb[i] : p.xa[i];
+        if (cur) p.xa[i] = xf;
+        if (p.finish) {
+            const float4 xp = p.xprev[i];
+            float4 vi = p.v[i];
+            vi.x = ((xf.x - xp.x) / p.h) * 0.999f;
+            vi.y = ((xf.y - xp.y) / p.h) * 0.999f;
+            vi.z = ((xf.z - xp.z) / p.h) * 0.999f;
+            p.v[i] = vi;
+        }
+    }
+}
+
+// ---- persistent colour walk with one CTA per SM ----------------------------------------------
+//
+// The same step as k_persistent, shaped to make the grid barrier cheap: one CTA of BLOCK threads per
+// SM (148 arrivals per barrier), a monotonic arrival counter that each CTA bumps with one
+// fire-and-forget add and then polls with acquire loads until it reaches the barrier's target, and
+// each CTA's first DEPTH records per lane of the colour after the barrier loaded before it waits.
+// Every CTA sweeps one contiguous share of each colour, LANES threads per vertex, in rounds of
+// BLOCK / LANES vertices.  Same arithmetic and summation order as k_sweep's deep prefetch, so the
+// same bits.  Shapes that fit without spilling: 768 threads with 3 records ahead (80 registers),
+// 1024 threads with 2 (64 registers, a few bytes of spill).
+
+// Barrier `index` (0, 1, 2, ...) of a launch whose counter started at zero: complete when all
+// `expected` CTAs have arrived index + 1 times.  Bounded: after spin_limit polls the CTA records
+// ST_TIMEOUT and the call returns false.
+__device__ __forceinline__ bool grid_sync_counted(unsigned* counter, unsigned index, int expected, long long spin_limit,
+                                                  unsigned long long* status) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned target = (index + 1u) * (unsigned)expected;
+        __threadfence();
+        asm volatile("red.relaxed.gpu.global.add.u32 [%0], 1;" ::"l"(counter) : "memory");
+        long long polls = 0;
+        while ((int)(ld_acquire_gpu(counter) - target) < 0) {
+            if (++polls > spin_limit) {
+                ok = 0;
+                atomicOr(reinterpret_cast<unsigned int*>(status + ST_TIMEOUT), 1u);
+                break;
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+
+// This CTA's share of colour range [vb, ve): [*b0, *b1).
+__device__ __forceinline__ void wave_share(int vb, int ve, int* b0, int* b1) {
+    const int n = ve - vb;
+    const int per = (n + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int s = vb + min(n, per * (int)blockIdx.x);
+    *b0 = s;
+    *b1 = min(ve, s + per);
+}
+
+template <int LANES, int LAYOUT, int DEPTH>
+struct WaveRound {
+    typename Elem<LAYOUT>::Rec buf[DEPTH];
+    int v, j, j1;
+    bool active;
+
+    // The round's vertex for this thread and its first records (element data never changes during
+    // a step, so they may be loaded before the barrier that precedes the round).
+    __device__ __forceinline__ void load(const SweepParams& p, int v0, int vend) {
+        const int lane = LANES == 1 ? 0 : (threadIdx.x & (LANES - 1));
+        v = v0 + (int)threadIdx.x / LANES;
+        active = v < vend;
+        int j0 = 0;
+        j1 = 0;
+        if (active) {
+            j0 = __ldg(p.inc_off + v);
+            j1 = __ldg(p.inc_off + v + 1);
+        }
+        j = j0 + lane;
+#pragma unroll
+        for (int k = 0; k < DEPTH; ++k)
+            if (j + k * LANES < j1) buf[k] = Elem<LAYOUT>::fetch(p, j + k * LANES);
+    }
+
+    __device__ __forceinline__ void run(const SweepParams& p) const {
+        const int lane = LANES == 1 ? 0 : (threadIdx.x & (LANES - 1));
+        const float4 xi = active ? p.x[v] : make_float4(0.f, 0.f, 0.f, 0.f);
+        Acc acc;
+        acc.zero();
+#pragma unroll
+        for (int k = 0; k < DEPTH; ++k)
+            if (j + k * LANES < j1) Elem<LAYOUT>::template contrib<true>(buf[k], v, xi, p.x, acc);
+        for (int jj = j + DEPTH * LANES; jj < j1; jj += LANES)
+            Elem<LAYOUT>::template contrib<true>(Elem<LAYOUT>::fetch(p, jj), v, xi, p.x, acc);
+        vertex_solve<LANES>(p, v, lane, active, xi, acc);
+    }
+};
+
+template <int LANES, int LAYOUT, int BLOCK, int DEPTH>
+__global__ void __launch_bounds__(BLOCK, 1) k_persist_wave(PersistParams p) {
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nthreads = gridDim.x * blockDim.x;
+    unsigned* counter = &p.bar->count;
+    unsigned bar_index = 0;
+    if (p.predict) {
+        for (int i = gtid; i < p.n; i += nthreads) {
+            const float4 xi = p.xa[i];
+            p.xprev[i] = xi;
+            float4 yi = p.sw.y[i];
+            if (i < p.nfree) {
+                float4 vi = p.v[i];
+                vi.x += p.hgx;
+                vi.y += p.hgy;
+                vi.z += p.hgz;
+                p.v[i] = vi;
+                yi.x = __fadd_rn(xi.x, __fmul_rn(p.h, vi.x));
+                yi.y = __fadd_rn(xi.y, __fmul_rn(p.h, vi.y));
+                yi.z = __fadd_rn(xi.z, __fmul_rn(p.h, vi.z));
+            } else {
+                yi.x = xi.x;
+                yi.y = xi.y;
+                yi.z = xi.z;
+            }
+            const_cast<float4*>(p.sw.y)[i] = yi;
+        }
+    }
+    if (p.init_from_inertia) {
+        for (int i = gtid; i < p.n; i += nthreads) {
+            const float4 yi = p.sw.y[i];
+            float4 a = p.xa[i], b = p.xb[i];
+            a.x = b.x = yi.x;
+            a.y = b.y = yi.y;
+            a.z = b.z = yi.z;
+            p.xa[i] = a;
+            p.xb[i] = b;
+        }
+    }
+    const int per_round = BLOCK / LANES;
+    WaveRound<LANES, LAYOUT, DEPTH> rnd;
+    int b0 = 0, b1 = 0;
+    if (p.iters > 0 && p.ncol > 0) {
+        wave_share(p.cstart[0], p.cstart[1], &b0, &b1);
+        rnd.load(p.sw, b0, b1);
+    }
+    if (!grid_sync_counted(counter, bar_index++, p.expected_blocks, p.spin_limit, p.sw.status)) return;
+
+    int cur = 0;
+    SweepParams sp = p.sw;
+    for (int k = 0; k < p.iters; ++k) {
+        const float om = p.omega[k];
+        const bool blend = om > 1.0f;
+        sp.x = cur ? p.xb : p.xa;
+        sp.xnext = cur ? p.xa : p.xb;
+        sp.omega = om;
+        sp.accel = blend ? 1 : 0;
+        for (int c = 0; c < p.ncol; ++c) {
+            // rounds of this CTA's share; the first was loaded before the barrier
+            for (int v0 = b0; v0 < b1; v0 += per_round) {
+                if (v0 != b0) rnd.load(sp, v0, b1);
+                rnd.run(sp);
+            }
+            // the next colour's (or the next iteration's first colour's) first round, before the wait
+            const bool last = (c + 1 == p.ncol) && (k + 1 == p.iters);
+            if (!last) {
+                const int cn = (c + 1) % p.ncol;
+                wave_share(p.cstart[cn], p.cstart[cn + 1], &b0, &b1);
+                rnd.load(sp, b0, b1);
+            }
+            if (!grid_sync_counted(counter, bar_index++, p.expected_blocks, p.spin_limit, p.sw.status)) return;
         }
         if (blend) cur ^= 1;
     }
@@ -1667,6 +1924,30 @@ __global__ void k_sum_partials(const double* __restrict__ partials, int n, doubl
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
         if (threadIdx.x == 0) out[0] = w;
+    }
+}
+
+// Sums partials[0..n) as k_sum_partials does and appends the sum to a history: hist[*count] when
+// *count < capacity; *count always advances, so a reader sees how many sums were produced.  One
+// block, so the append needs no atomics.
+__global__ void k_sum_partials_append(const double* __restrict__ partials, int n, double* __restrict__ hist,
+                                      int* __restrict__ count, int capacity) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += partials[i];
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double w = threadIdx.x < (int)(blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if (threadIdx.x == 0) {
+            const int k = *count;
+            if (k < capacity) hist[k] = w;
+            *count = k + 1;
+        }
     }
 }
 

@@ -67,34 +67,36 @@ static float omega_of_wrapper(int order, float rho, float prev) {
 
 using SweepFn = void (*)(SweepParams);
 
-// prefetch 0 / 1 / 2 = k_sweep's PREFETCH 0 / 1 / 3 (deep prefetch for the factored layouts only;
-// the others run PREFETCH 1 for option 2).  The factored layouts' PREFETCH 1 runs as
-// k_sweep_capped (56 registers).
-template <int L, int LAYOUT> static SweepFn pick_depth(int prefetch) {
-    if (prefetch == 0) return &k_sweep<L, LAYOUT, 0>;
-    if (LAYOUT >= 3 && L > 1 && prefetch == 1) return &k_sweep_capped<L, LAYOUT>;
-    if (prefetch == 1 || LAYOUT < 3) return &k_sweep<L, LAYOUT, 1>;
-    return &k_sweep<L, LAYOUT, (LAYOUT < 3 ? 1 : 3)>;
+// prefetch 0 / 1 / 2 / 3 = k_sweep's PREFETCH 0 / 1 / 3 and k_sweep_capped's PREFETCH 2 (the deep
+// forms for the factored layouts only; the others run PREFETCH 1 for options 2 and 3).  The
+// factored layouts' PREFETCH 1 runs as k_sweep_capped (56 registers).  `cache` selects the
+// record loads with an L2 policy (factored layouts; k_sweep's CACHE).
+template <int L, int LAYOUT, bool CACHE> static SweepFn pick_depth(int prefetch) {
+    if (prefetch == 0) return &k_sweep<L, LAYOUT, 0, CACHE>;
+    if (LAYOUT >= 3 && L > 1 && prefetch == 1) return &k_sweep_capped<L, LAYOUT, 1, CACHE>;
+    if (prefetch == 1 || LAYOUT < 3) return &k_sweep<L, LAYOUT, 1, CACHE>;
+    if (prefetch == 3 && L > 1) return &k_sweep_capped<L, LAYOUT, 2, CACHE>;
+    return &k_sweep<L, LAYOUT, (LAYOUT < 3 ? 1 : 3), CACHE>;
 }
 
-template <int L> static SweepFn pick_sweep(int layout, int prefetch) {
+template <int L> static SweepFn pick_sweep(int layout, int prefetch, bool cache) {
     switch (layout) {
-        case 0: return pick_depth<L, 0>(prefetch);
-        case 1: return pick_depth<L, 1>(prefetch);
-        case 2: return pick_depth<L, 2>(prefetch);
-        case 3: return pick_depth<L, 3>(prefetch);
-        default: return pick_depth<L, 4>(prefetch);
+        case 0: return pick_depth<L, 0, false>(prefetch);
+        case 1: return pick_depth<L, 1, false>(prefetch);
+        case 2: return pick_depth<L, 2, false>(prefetch);
+        case 3: return cache ? pick_depth<L, 3, true>(prefetch) : pick_depth<L, 3, false>(prefetch);
+        default: return cache ? pick_depth<L, 4, true>(prefetch) : pick_depth<L, 4, false>(prefetch);
     }
 }
 
-static SweepFn pick_sweep(int lanes, int layout, int prefetch) {
+static SweepFn pick_sweep(int lanes, int layout, int prefetch, bool cache) {
     switch (lanes) {
-        case 1: return pick_sweep<1>(layout, prefetch);
-        case 2: return pick_sweep<2>(layout, prefetch);
-        case 4: return pick_sweep<4>(layout, prefetch);
-        case 8: return pick_sweep<8>(layout, prefetch);
-        case 16: return pick_sweep<16>(layout, prefetch);
-        default: return pick_sweep<32>(layout, prefetch);
+        case 1: return pick_sweep<1>(layout, prefetch, cache);
+        case 2: return pick_sweep<2>(layout, prefetch, cache);
+        case 4: return pick_sweep<4>(layout, prefetch, cache);
+        case 8: return pick_sweep<8>(layout, prefetch, cache);
+        case 16: return pick_sweep<16>(layout, prefetch, cache);
+        default: return pick_sweep<32>(layout, prefetch, cache);
     }
 }
 
@@ -106,6 +108,13 @@ template <int L> static void (*pick_persistent(int layout))(PersistParams) {
         case 3: return &k_persistent<L, 3>;
         default: return &k_persistent<L, 4>;
     }
+}
+
+// The one-CTA-per-SM persistent kernel (factored layouts only): VBD_OPT_PERSISTENT 2 runs 768-thread
+// CTAs with 3 records ahead, 3 runs 1024-thread CTAs with 2.
+template <int L> static void (*pick_persist_wave(int layout, int kind))(PersistParams) {
+    if (kind == 2) return layout == 3 ? &k_persist_wave<L, 3, 768, 3> : &k_persist_wave<L, 4, 768, 3>;
+    return layout == 3 ? &k_persist_wave<L, 3, 1024, 2> : &k_persist_wave<L, 4, 1024, 2>;
 }
 
 // The adjoint reads tet records (layouts 0 and 1) or the forward's streamed incidence records.
@@ -122,6 +131,7 @@ template <int L> static void (*pick_adj_sweep(int layout))(AdjParams) {
 struct GraphKey {
     int kind;  // 0 = step, 1 = solve, 2 = single sweep
     int iters, accel, init, lanes, layout, prefetch, pdl, block, semantics, l2_prefetch, src;
+    int record_cache, persist_mb, shape_gen, energy_every;
     float h, dtsr, hg[3], rho;
     bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
 };
@@ -170,6 +180,22 @@ struct vbd_solver {
     // Off by default: on the 64^3 cube it measured 5.48 against 4.78 ms/step (the extra DRAM
     // traffic competes with the running colour's own stream).
     int l2_prefetch = 0;
+    // VBD_OPT_RECORD_CACHE: the factored records are loaded with an L2 policy, evict-first except
+    // the first persist_mb megabytes of the record stream (VBD_OPT_RECORD_PERSIST_MB), which are
+    // loaded evict-last so that they stay in L2 from one sweep to the next.
+    int record_cache = 0, persist_mb = 0;
+    // Per-colour threads per vertex (vbd_solver_set_colour_lanes); empty = `lanes` for every colour.
+    // shape_gen changes with every setting, so captured graphs of another shape are not reused.
+    std::vector<int> colour_lanes;
+    std::vector<int> colour_maxval;     // most incident tets of a free vertex, per colour
+    int shape_gen = 0;
+    // VBD_OPT_ENERGY_EVERY: vbd_solver_step appends VBDsolver::computeTotalEnergy after iterations
+    // 0, k, 2k, ... of every sub-step (VBD.cpp:93-95 with k = 10) to a device-side history, read by
+    // vbd_solver_energy_history.  ehist_queued counts the values enqueued since the last reset.
+    int energy_every = 0;
+    vbd::DBuf<double> ehist;
+    vbd::DBuf<int> ecount;
+    long long ehist_queued = 0;
     std::vector<long long> colour_inc;  // first incidence of each colour (C + 1 entries)
     // VBD_OPT_SEMANTICS: 0 = VBDsolver (VBD.cpp), 1 = VBD_GPU_Solver (VBD_GPU_Wrapper.cu)
     int semantics = 0;
@@ -256,9 +282,73 @@ struct vbd_solver {
     // against 4.55 ms/step; on the 512-mesh batch (4 lanes, up to 6): 7.72 against 7.44 (both
     // before PREFETCH 1 was held to 56 registers, which brought the cube to 4.48 and the batch to
     // 7.10).
-    int eff_prefetch() const {
+    int eff_prefetch() const { return prefetch_for(lanes, max_valence); }
+    int prefetch_for(int L, int maxval) const {
         if (!prefetch_auto) return prefetch;
-        return (layout == 4 && lanes > 0 && (max_valence + lanes - 1) / lanes <= 3) ? 2 : 1;
+        return (layout == 4 && L > 0 && (maxval + L - 1) / L <= 3) ? 2 : 1;
+    }
+    int lanes_of(int c) const { return colour_lanes.empty() ? lanes : colour_lanes[c]; }
+    int prefetch_of(int c) const {
+        return colour_lanes.empty() ? eff_prefetch() : prefetch_for(colour_lanes[c], colour_maxval[c]);
+    }
+    // First incidence whose record is loaded evict-first (records before it evict-last).
+    int persist_end() const {
+        if (!record_cache || persist_mb <= 0) return 0;
+        const double rec_bytes = layout == 4 ? 40.0 : 48.0;
+        const double n = (double)persist_mb * 1048576.0 / rec_bytes;
+        return (int)std::min<double>(n, (double)ninc);
+    }
+    // The launch-shape fields of a graph key.
+    void shape_key(vbd::GraphKey& key) const {
+        key.lanes = lanes;
+        key.layout = layout;
+        key.prefetch = eff_prefetch();
+        key.pdl = pdl;
+        key.block = block;
+        key.semantics = semantics;
+        key.l2_prefetch = l2_prefetch;
+        key.record_cache = record_cache;
+        key.persist_mb = persist_mb;
+        key.shape_gen = shape_gen;
+        key.energy_every = energy_every;
+    }
+
+    // Energies a step of `substeps` x `iters` appends to the history.
+    long long energies_per_step(int substeps, int iters) const {
+        if (energy_every <= 0 || iters <= 0) return 0;
+        return (long long)substeps * ((iters + energy_every - 1) / energy_every);
+    }
+
+    // Room in the history for `more` values after those already queued; a larger buffer keeps the
+    // queued values (captured graphs bake the buffer's address, so they are dropped).
+    int reserve_energies(long long more) {
+        if (!ecount.p) {
+            VBD_TRY(ecount.alloc(1));
+            CUDA_TRY(cudaMemsetAsync(ecount.p, 0, sizeof(int), stream));
+        }
+        const long long need = ehist_queued + more;
+        if (need <= (long long)ehist.n) return VBD_OK;
+        if (need > 0x7fffffffLL) VBD_FAIL(VBD_ERR_INVALID_ARG, "energy history is full: read it with reset");
+        vbd::DBuf<double> bigger;
+        VBD_TRY(bigger.alloc((size_t)std::max<long long>(2 * need, 64)));
+        if (ehist_queued > 0 && ehist.p)
+            CUDA_TRY(cudaMemcpyAsync(bigger.p, ehist.p, sizeof(double) * (size_t)std::min<long long>(ehist_queued, ehist.n),
+                                     cudaMemcpyDeviceToDevice, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        drop_graphs();
+        std::swap(ehist.p, bigger.p);
+        std::swap(ehist.n, bigger.n);
+        return VBD_OK;
+    }
+
+    // VBDsolver::computeTotalEnergy (log-J elastic energy, FP64 sums) of positions X, appended to
+    // the history.
+    int emit_energy_append(const float4* X) {
+        const unsigned blocks = std::max(1u, std::min<unsigned>(vbd::nblk(T, 256), 4096u));
+        vbd::k_energy<<<blocks, 256, 0, stream>>>(X, y.p, rec.p, 0, T, 1, 0.0, partials.p);
+        VBD_TRY(check_launch());
+        vbd::k_sum_partials_append<<<1, 1024, 0, stream>>>(partials.p, (int)blocks, ehist.p, ecount.p, (int)ehist.n);
+        return check_launch();
     }
 
     int check_launch() {
@@ -273,7 +363,7 @@ struct vbd_solver {
         if (ve <= vb) return VBD_OK;
         vbd::SweepParams p{xr,     xn,     pp.p,     y.p, inc_off.p, inc_tet.p, rec.p,          irec.p,
                            crec.p, cmat.p, status.p, vb,  ve,        dtsr,      omega, accel ? 1 : 0,
-                           keep_pp ? 1 : 0, nullptr};
+                           keep_pp ? 1 : 0, persist_end(), 0};
         if (l2_prefetch && layout >= 2 && crec.p && C > 0) {
             // the colour swept after this one (colour 0 of the next iteration after the last)
             const int cn = (c + 1) % C;
@@ -282,8 +372,9 @@ struct vbd_solver {
             p.l2_next = reinterpret_cast<const char*>(crec.p + words * j0);
             p.l2_bytes = (unsigned long long)(j1 - j0) * 16ull * words;
         }
-        long long threads = (long long)(ve - vb) * lanes;
-        vbd::SweepFn fn = vbd::pick_sweep(lanes, layout, eff_prefetch());
+        const int L = lanes_of(c);
+        long long threads = (long long)(ve - vb) * L;
+        vbd::SweepFn fn = vbd::pick_sweep(L, layout, prefetch_of(c), record_cache != 0);
         int threads_per_block = block;
         if (semantics) threads = (long long)(ve - vb) * vbd::kWrapperLanes;
         cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -319,8 +410,10 @@ struct vbd_solver {
         return VBD_OK;
     }
 
-    // `iters` sweeps with the Chebyshev schedule; `cur` tracks which buffer holds x.
-    int emit_iterations(int iters, float dtsr, bool accel, float rho, int& cur) {
+    // `iters` sweeps with the Chebyshev schedule; `cur` tracks which buffer holds x.  With
+    // record_energy, the log-J energy of the blended positions is appended after iterations 0, k,
+    // 2k, ... (k = energy_every), where VBDsolver::step evaluates it (VBD.cpp:93-95).
+    int emit_iterations(int iters, float dtsr, bool accel, float rho, int& cur, bool record_energy = false) {
         float omega = 1.0f;
         for (int k = 1; k <= iters; ++k) {
             bool blend = false;
@@ -332,11 +425,14 @@ struct vbd_solver {
             float4* xo = cur ? x0.p : x1.p;
             for (int c = 0; c < C; ++c) VBD_TRY(launch_sweep(c, xr, xo, blend, accel, dtsr, omega));
             if (blend) cur ^= 1;
+            if (record_energy && energy_every > 0 && (k - 1) % energy_every == 0)
+                VBD_TRY(emit_energy_append(cur ? x1.p : x0.p));
         }
         return VBD_OK;
     }
 
-    int emit_substep(float h, float dtsr, const float* hg, int iters, bool accel, float rho) {
+    int emit_substep(float h, float dtsr, const float* hg, int iters, bool accel, float rho,
+                     bool record_energy = false) {
         vbd::k_predict<<<vbd::nblk(N, 256), 256, 0, stream>>>(x0.p, v.p, xprev.p, y.p, nfree, N, h, hg[0], hg[1],
                                                               hg[2]);
         VBD_TRY(check_launch());
@@ -347,7 +443,7 @@ struct vbd_solver {
             VBD_TRY(check_launch());
         }
         int cur = 0;
-        VBD_TRY(emit_iterations(iters, dtsr, accel, rho, cur));
+        VBD_TRY(emit_iterations(iters, dtsr, accel, rho, cur, record_energy));
         if (nfree > 0) {
             vbd::k_finish<<<vbd::nblk(nfree, 256), 256, 0, stream>>>(cur ? x1.p : x0.p, x0.p, xprev.p, v.p, nfree, h,
                                                                      cur, 1);
@@ -396,21 +492,28 @@ struct vbd_solver {
             omega_cache = w;
         }
         const int L = lanes < 4 ? 4 : lanes;
+        // persistent 2 / 3: one CTA per SM with the counted barrier (factored layouts)
+        const bool wave = persistent >= 2 && layout >= 3;
+        const int threads = wave ? (persistent == 2 ? 768 : 1024) : 256;
         void (*fn)(vbd::PersistParams) = nullptr;
         switch (L) {
-            case 4: fn = vbd::pick_persistent<4>(layout); break;
-            case 8: fn = vbd::pick_persistent<8>(layout); break;
-            case 16: fn = vbd::pick_persistent<16>(layout); break;
-            default: fn = vbd::pick_persistent<32>(layout); break;
+            case 4: fn = wave ? vbd::pick_persist_wave<4>(layout, persistent) : vbd::pick_persistent<4>(layout); break;
+            case 8: fn = wave ? vbd::pick_persist_wave<8>(layout, persistent) : vbd::pick_persistent<8>(layout); break;
+            case 16:
+                fn = wave ? vbd::pick_persist_wave<16>(layout, persistent) : vbd::pick_persistent<16>(layout);
+                break;
+            default:
+                fn = wave ? vbd::pick_persist_wave<32>(layout, persistent) : vbd::pick_persistent<32>(layout);
+                break;
         }
         int per_sm = 0, sms = 0;
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0));
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0));
         CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
         if (per_sm < 1) VBD_FAIL(VBD_ERR_CUDA, "persistent kernel cannot be resident");
         const int grid = per_sm * sms;
         vbd::PersistParams pp_{};
         pp_.sw = vbd::SweepParams{x0.p, x1.p, pp.p, y.p,  inc_off.p, inc_tet.p, rec.p, irec.p, crec.p, cmat.p,
-                                  status.p, 0,  0,    dtsr, 1.0f,      0,         accel ? 1 : 0, nullptr};
+                                  status.p, 0,  0,    dtsr, 1.0f,      0,         accel ? 1 : 0, 0, 0};
         pp_.xa = x0.p;
         pp_.xb = x1.p;
         pp_.v = v.p;
@@ -433,7 +536,7 @@ struct vbd_solver {
         pp_.hgz = hg ? hg[2] : 0.f;
         CUDA_TRY(cudaMemsetAsync(barrier.p, 0, sizeof(vbd::GridBarrier), stream));
         void* args[] = {&pp_};
-        CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(fn), dim3(grid), dim3(256), args, 0, stream));
+        CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(fn), dim3(grid), dim3(threads), args, 0, stream));
         return check_launch();
     }
 
@@ -465,13 +568,8 @@ struct vbd_solver {
         key.kind = 0;
         key.iters = t.iters;
         key.accel = t.accel;
-        key.lanes = lanes;
-        key.layout = layout;
-        key.prefetch = eff_prefetch();
-        key.pdl = pdl;
-        key.block = block;
-        key.semantics = semantics;
-        key.l2_prefetch = l2_prefetch;
+        shape_key(key);
+        key.energy_every = 0;  // the recompute appends no energies (the sweeps, hence the bits, are the same)
         key.h = t.h;
         key.dtsr = t.dtsr;
         key.hg[0] = t.hg[0];
@@ -890,6 +988,9 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     CUDA_TRY(cudaMemcpy(s->inc_vertex.p, inc_vertex.data(), sizeof(int) * inc_vertex.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->rec.p, rec.data(), sizeof(vbd::TetRec) * rec.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemset(s->status.p, 0, sizeof(unsigned long long) * vbd::ST_SLOTS));
+    // the energy history belongs to the previous mesh
+    s->ehist_queued = 0;
+    if (s->ecount.p) CUDA_TRY(cudaMemset(s->ecount.p, 0, sizeof(int)));
 
     if (s->lanes_auto) {
         int L = (nfree > 0 && (double)ninc >= 21.0 * nfree) ? 8 : 4;
@@ -903,6 +1004,13 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     if (s->layout_auto) s->layout = N <= vbd::kPackedMaxVertices ? 4 : 3;
     s->max_valence = 0;
     for (int i = 0; i < nfree; ++i) s->max_valence = std::max(s->max_valence, inc_off[i + 1] - inc_off[i]);
+    s->colour_maxval.assign(num_colours, 0);
+    for (int c = 0; c < num_colours; ++c)
+        for (int i = cstart[c]; i < cstart[c + 1]; ++i)
+            s->colour_maxval[c] = std::max(s->colour_maxval[c], inc_off[i + 1] - inc_off[i]);
+    // a per-colour launch shape belongs to the previous mesh's colours
+    s->colour_lanes.clear();
+    ++s->shape_gen;
     s->colour_inc.assign(num_colours + 1, 0);
     for (int c = 0; c <= num_colours; ++c) s->colour_inc[c] = inc_off[cstart[c]];
     s->colour_bytes.assign(num_colours, 0.0);
@@ -1069,13 +1177,7 @@ int vbd_solver_solve(vbd_solver* s, int32_t iterations, float dt_sqr_reciprocal,
     key.iters = iterations;
     key.accel = use_acceleration ? 1 : 0;
     key.init = init_mode;
-    key.lanes = s->lanes;
-    key.layout = s->layout;
-    key.prefetch = s->eff_prefetch();
-    key.pdl = s->pdl;
-    key.block = s->block;
-    key.semantics = s->semantics;
-    key.l2_prefetch = s->l2_prefetch;
+    s->shape_key(key);
     key.dtsr = dt_sqr_reciprocal;
     key.rho = rho;
     if (s->persistent && !s->timing)
@@ -1113,25 +1215,52 @@ int vbd_solver_step(vbd_solver* s, float dt, int32_t substeps, int32_t iteration
     key.kind = 0;
     key.iters = iterations;
     key.accel = use_acceleration ? 1 : 0;
-    key.lanes = s->lanes;
-    key.layout = s->layout;
-    key.prefetch = s->eff_prefetch();
-    key.pdl = s->pdl;
-    key.block = s->block;
-    key.semantics = s->semantics;
-    key.l2_prefetch = s->l2_prefetch;
+    s->shape_key(key);
     key.h = h;
     key.dtsr = dtsr;
     key.hg[0] = hg[0];
     key.hg[1] = hg[1];
     key.hg[2] = hg[2];
     key.rho = rho;
+    const long long nenergy = s->energies_per_step(substeps, iterations);
+    if (nenergy > 0) VBD_TRY(s->reserve_energies(nenergy));
     for (int k = 0; k < substeps; ++k) {
-        if (s->persistent && !s->timing)
+        // the persistent kernel evaluates no energies: with an energy history the step runs as
+        // separate launches
+        if (s->persistent && !s->timing && nenergy == 0)
             VBD_TRY(s->launch_persistent(iterations, dtsr, use_acceleration != 0, rho, true, true, false, h, hg));
         else
-            VBD_TRY(s->run(key, [&] { return s->emit_substep(h, dtsr, hg, iterations, use_acceleration != 0, rho); }));
+            VBD_TRY(s->run(key, [&] {
+                return s->emit_substep(h, dtsr, hg, iterations, use_acceleration != 0, rho, nenergy > 0);
+            }));
         VBD_TRY(s->record_substep(h, dtsr, hg, iterations, use_acceleration != 0, rho));
+    }
+    s->ehist_queued += nenergy;
+    return VBD_OK;
+}
+
+int vbd_solver_energy_history(vbd_solver* s, double* energies, int32_t capacity, int32_t* count, int32_t reset) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!count) VBD_FAIL(VBD_ERR_INVALID_ARG, "count is null");
+    if (capacity < 0 || (capacity > 0 && !energies)) VBD_FAIL(VBD_ERR_INVALID_ARG, "need energies[capacity]");
+    DeviceScope scope(s->device);
+    int n = 0;
+    if (s->ecount.p) {
+        CUDA_TRY(cudaMemcpyAsync(&n, s->ecount.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+    }
+    const int avail = (int)std::min<long long>(n, (long long)s->ehist.n);
+    const int copy = std::min(avail, capacity);
+    if (copy > 0) {
+        CUDA_TRY(cudaMemcpyAsync(energies, s->ehist.p, sizeof(double) * copy, cudaMemcpyDefault, s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+    }
+    *count = n;
+    if (reset && s->ecount.p) {
+        CUDA_TRY(cudaMemsetAsync(s->ecount.p, 0, sizeof(int), s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+        s->ehist_queued = 0;
     }
     return VBD_OK;
 }
@@ -1292,7 +1421,7 @@ int vbd_solver_energy(vbd_solver* s, int32_t kind, float h, double* out) {
         }
         vbd::SweepParams p{s->x0.p,     nullptr, s->pp.p,    s->y.p, s->inc_off.p, s->inc_tet.p,
                            s->rec.p,    s->irec.p, s->crec.p, s->cmat.p, s->status.p, 0,
-                           s->nfree,    (float)(1.0 / ((double)h * h)), 1.0f, 0, 0, nullptr};
+                           s->nfree,    (float)(1.0 / ((double)h * h)), 1.0f, 0, 0, 0, 0};
         const int L = std::max(4, s->lanes);
         const unsigned blocks = vbd::nblk((long long)s->nfree * L, 256);
         switch (L) {
@@ -1344,9 +1473,20 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
             s->lanes_auto = false;
             return VBD_OK;
         case VBD_OPT_PREFETCH:
-            if (value < 0 || value > 2) VBD_FAIL(VBD_ERR_INVALID_ARG, "prefetch must be 0, 1 or 2");
+            if (value < 0 || value > 3) VBD_FAIL(VBD_ERR_INVALID_ARG, "prefetch must be 0, 1, 2 or 3");
             s->prefetch = value;
             s->prefetch_auto = false;
+            return VBD_OK;
+        case VBD_OPT_RECORD_CACHE:
+            s->record_cache = value ? 1 : 0;
+            return VBD_OK;
+        case VBD_OPT_RECORD_PERSIST_MB:
+            if (value < 0) VBD_FAIL(VBD_ERR_INVALID_ARG, "persist megabytes must be >= 0");
+            s->persist_mb = value;
+            return VBD_OK;
+        case VBD_OPT_ENERGY_EVERY:
+            if (value < 0) VBD_FAIL(VBD_ERR_INVALID_ARG, "energy interval must be >= 0");
+            s->energy_every = value;
             return VBD_OK;
         case VBD_OPT_PDL:
             s->pdl = value ? 1 : 0;
@@ -1354,7 +1494,8 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
         case VBD_OPT_PERSISTENT:
             if (value && s->semantics)
                 VBD_FAIL(VBD_ERR_INVALID_ARG, "the persistent kernel runs the VBDsolver semantics only");
-            s->persistent = value ? 1 : 0;
+            if (value < 0 || value > 3) VBD_FAIL(VBD_ERR_INVALID_ARG, "persistent must be 0, 1, 2 or 3");
+            s->persistent = value;
             return VBD_OK;
         case VBD_OPT_L2_PREFETCH:
             s->l2_prefetch = value ? 1 : 0;
@@ -1412,8 +1553,39 @@ int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value) {
         case VBD_OPT_SEMANTICS: *value = s->semantics; return VBD_OK;
         case VBD_OPT_L2_PREFETCH: *value = s->l2_prefetch; return VBD_OK;
         case VBD_OPT_ADJOINT_ALTERNATE: *value = s->adj_alternate; return VBD_OK;
+        case VBD_OPT_RECORD_CACHE: *value = s->record_cache; return VBD_OK;
+        case VBD_OPT_RECORD_PERSIST_MB: *value = s->persist_mb; return VBD_OK;
+        case VBD_OPT_ENERGY_EVERY: *value = s->energy_every; return VBD_OK;
         default: VBD_FAIL(VBD_ERR_INVALID_ARG, "unknown option %d", option);
     }
+}
+
+int vbd_solver_set_colour_lanes(vbd_solver* s, int32_t num_colours, const int32_t* lanes) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!lanes) {
+        s->colour_lanes.clear();
+        ++s->shape_gen;
+        return VBD_OK;
+    }
+    if (num_colours != s->C) VBD_FAIL(VBD_ERR_INVALID_ARG, "need one lane count per colour (%d), got %d", s->C, num_colours);
+    for (int c = 0; c < num_colours; ++c) {
+        const int v = lanes[c];
+        if (v != 1 && v != 2 && v != 4 && v != 8 && v != 16 && v != 32)
+            VBD_FAIL(VBD_ERR_INVALID_ARG, "colour %d: lanes must be 1, 2, 4, 8, 16 or 32 (got %d)", c, v);
+    }
+    s->colour_lanes.assign(lanes, lanes + num_colours);
+    ++s->shape_gen;
+    return VBD_OK;
+}
+
+int vbd_solver_get_colour_lanes(vbd_solver* s, int32_t num_colours, int32_t* lanes) {
+    vbd::clear_error();
+    VBD_TRY(need_ready(s));
+    if (!lanes || num_colours != s->C)
+        VBD_FAIL(VBD_ERR_INVALID_ARG, "need an array of one entry per colour (%d)", s->C);
+    for (int c = 0; c < num_colours; ++c) lanes[c] = s->lanes_of(c);
+    return VBD_OK;
 }
 
 int vbd_solver_info(vbd_solver* s, int32_t* num_verts, int32_t* num_tets, int32_t* num_colours) {
@@ -1459,53 +1631,108 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
     CUDA_TRY(cudaMemcpyAsync(st, s->status.p, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     const int saved_timing = s->timing;
+    const int saved_energy = s->energy_every;
     s->timing = 0;
+    s->energy_every = 0;  // the candidate steps append no energies
+    // The whole launch configuration a candidate sets.
     struct Cand {
-        int lanes, layout, prefetch, pdl, block;
-    };
-    static const Cand cands[] = {
-        {8, 4, 2, 1, 64}, {8, 4, 1, 1, 64}, {8, 4, 1, 1, 128}, {4, 4, 1, 1, 128}, {16, 4, 2, 1, 64},
-        {16, 4, 1, 1, 64}, {8, 4, 0, 1, 64},
-        {8, 3, 1, 1, 64}, {8, 3, 1, 1, 128}, {4, 3, 1, 1, 128}, {16, 3, 1, 1, 64}, {8, 3, 0, 1, 64},
-        {8, 3, 1, 0, 64}, {4, 2, 1, 1, 128}, {8, 2, 1, 1, 64},  {2, 2, 1, 1, 128}, {8, 1, 1, 1, 128},
-        {8, 0, 1, 1, 128}, {4, 0, 1, 1, 128},
+        int lanes, layout, prefetch, pdl, block, persistent, cache;
+        std::vector<int> colour_lanes;  // empty = `lanes` for every colour
     };
     const float g[3] = {0.f, 0.f, 0.f};
     cudaEvent_t e0, e1;
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
-    float best_ms = 1e30f;
-    Cand best = {s->lanes, s->layout, s->eff_prefetch(), s->pdl, s->block};
-    s->prefetch_auto = false;
-    int rc = VBD_OK;
-    for (const Cand& c : cands) {
-        if (c.layout == 4 && s->N > vbd::kPackedMaxVertices) continue;
+    auto apply = [&](const Cand& c) -> int {
         s->lanes = c.lanes;
         s->prefetch = c.prefetch;
         s->pdl = c.pdl;
         s->block = c.block;
+        s->persistent = c.persistent;
+        s->record_cache = c.cache;
+        if (s->colour_lanes != c.colour_lanes) {
+            s->colour_lanes = c.colour_lanes;
+            ++s->shape_gen;
+        }
         if (s->layout != c.layout) {
             s->layout = c.layout;
-            if ((rc = s->repack_stream())) break;
+            return s->repack_stream();
         }
-        // one warm-up step (captures the graph), then the timed ones
-        if ((rc = vbd_solver_step(s, dt, 1, iterations, g, 1, 0.9f))) break;
-        cudaEventRecord(e0, s->stream);
-        for (int r = 0; r < repeats && !rc; ++r) rc = vbd_solver_step(s, dt, 1, iterations, g, 1, 0.9f);
-        cudaEventRecord(e1, s->stream);
-        if (rc) break;
-        if (cudaEventSynchronize(e1) != cudaSuccess) {
-            rc = VBD_ERR_CUDA;
-            break;
-        }
+        return VBD_OK;
+    };
+    // device time of `repeats` steps after one warm-up step (which captures the graph); the
+    // simulation state is restored afterwards
+    auto time_of = [&](const Cand& c, float* ms) -> int {
+        VBD_TRY(apply(c));
+        VBD_TRY(vbd_solver_step(s, dt, 1, iterations, g, 1, 0.9f));
+        CUDA_TRY(cudaEventRecord(e0, s->stream));
+        for (int r = 0; r < repeats; ++r) VBD_TRY(vbd_solver_step(s, dt, 1, iterations, g, 1, 0.9f));
+        CUDA_TRY(cudaEventRecord(e1, s->stream));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        VBD_TRY(vbd_solver_sync(s));  // a persistent barrier that gave up makes the candidate fail
+        CUDA_TRY(cudaEventElapsedTime(ms, e0, e1));
+        for (int k = 0; k < 6; ++k)
+            CUDA_TRY(cudaMemcpyAsync(bufs[k], save.p + (size_t)k * s->N, b4, cudaMemcpyDeviceToDevice, s->stream));
+        return VBD_OK;
+    };
+    // Phase 1: uniform launch shapes (threads per vertex, record layout, prefetch, PDL, block).
+    static const int uniform[][5] = {
+        {8, 4, 2, 1, 64}, {8, 4, 3, 1, 64}, {8, 4, 1, 1, 64}, {8, 4, 1, 1, 128}, {4, 4, 1, 1, 128},
+        {16, 4, 2, 1, 64}, {16, 4, 1, 1, 64}, {8, 4, 0, 1, 64},
+        {8, 3, 1, 1, 64}, {8, 3, 1, 1, 128}, {4, 3, 1, 1, 128}, {16, 3, 1, 1, 64}, {8, 3, 0, 1, 64},
+        {8, 3, 1, 0, 64}, {4, 2, 1, 1, 128}, {8, 2, 1, 1, 64},  {2, 2, 1, 1, 128}, {8, 1, 1, 1, 128},
+        {8, 0, 1, 1, 128}, {4, 0, 1, 1, 128},
+    };
+    Cand best{s->lanes, s->layout, s->eff_prefetch(), s->pdl, s->block, s->persistent, s->record_cache, s->colour_lanes};
+    float best_ms = 1e30f;
+    s->prefetch_auto = false;
+    int rc = VBD_OK;
+    for (const auto& u : uniform) {
+        if (u[1] == 4 && s->N > vbd::kPackedMaxVertices) continue;
+        Cand c{u[0], u[1], u[2], u[3], u[4], 0, 0, {}};
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
+        if ((rc = time_of(c, &ms))) break;
         if (ms < best_ms) {
             best_ms = ms;
             best = c;
         }
-        for (int k = 0; k < 6; ++k)
-            cudaMemcpyAsync(bufs[k], save.p + (size_t)k * s->N, b4, cudaMemcpyDeviceToDevice, s->stream);
+    }
+    // A later phase replaces the choice only when it is faster by more than 1% (timing noise).
+    auto try_cand = [&](const Cand& c) -> int {
+        float ms = 0.f;
+        VBD_TRY(time_of(c, &ms));
+        if (ms < 0.99f * best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+        return VBD_OK;
+    };
+    // Phase 2: the factored records' L2 policy (evict-first stream).
+    if (!rc && best.layout >= 3) {
+        Cand c = best;
+        c.cache = 1;
+        rc = try_cand(c);
+    }
+    // Phase 3: per-colour threads per vertex, greedily colour by colour (half, same, double).
+    if (!rc && s->semantics == 0 && s->C > 1) {
+        for (int col = 0; col < s->C && !rc; ++col) {
+            for (int f : {-1, 1}) {
+                Cand c = best;
+                if (c.colour_lanes.empty()) c.colour_lanes.assign(s->C, c.lanes);
+                const int L = f < 0 ? c.colour_lanes[col] / 2 : c.colour_lanes[col] * 2;
+                if (L < 2 || L > 32) continue;
+                c.colour_lanes[col] = L;
+                if ((rc = try_cand(c))) break;
+            }
+        }
+    }
+    // Phase 4: the whole step as one persistent colour-walking launch (uniform lanes, no per-colour
+    // shape) against the captured graph.
+    if (!rc && s->semantics == 0) {
+        Cand c = best;
+        c.persistent = 1;
+        c.colour_lanes.clear();
+        rc = try_cand(c);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1513,16 +1740,11 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
         CUDA_TRY(cudaMemcpyAsync(bufs[k], save.p + (size_t)k * s->N, b4, cudaMemcpyDeviceToDevice, s->stream));
     CUDA_TRY(cudaMemcpyAsync(s->status.p, st, sizeof(st), cudaMemcpyHostToDevice, s->stream));
     s->timing = saved_timing;
-    s->lanes = best.lanes;
-    s->prefetch = best.prefetch;
-    s->pdl = best.pdl;
-    s->block = best.block;
-    if (s->layout != best.layout) {
-        s->layout = best.layout;
-        VBD_TRY(s->repack_stream());
-    }
+    s->energy_every = saved_energy;
+    const int arc = apply(best);
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     if (rc) return rc;
+    if (arc) return arc;
     if (chosen) {
         chosen[0] = best.lanes;
         chosen[1] = best.layout;

@@ -4,7 +4,8 @@ Every mesh of the batch advances in one solver (colour c of all meshes in one la
 recorded forward and one backward pass (vbd_solver_record / vbd_solver_backward) give the
 per-tet gradients dL/dmu, dL/dlambda of the loss L = sum_m sum_i |x_i - x*_i|^2, which chain to
 each mesh's (log E, nu) through mu = E / (2 (1 + nu)), lambda = E nu / ((1 + nu)(1 - 2 nu)).
-Gradient descent (Adam) updates all meshes at once.  Finite-difference checks need only two
+Each mesh's (log E, nu) moves by its own quasi-Newton step with a line search (identify); a line
+search trial of all meshes costs one batched forward + adjoint.  Finite-difference checks need only two
 batched forwards per parameter, since the meshes are independent.
 """
 from __future__ import annotations
@@ -124,7 +125,74 @@ class Problem:
         return (Lp - Lm) / (2.0 * d)
 
 
-def identify(problem, targets, logE0, nu0, outer=50, lr_logE=0.15, lr_nu=0.01, nu_bounds=(0.05, 0.48)):
+NU_SCALE = 0.1  # nu is optimised as nu / NU_SCALE, so both coordinates move on similar scales
+
+
+def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), max_step=(1.0, 0.5), tries=6,
+             armijo=1e-4):
+    """Per-mesh quasi-Newton descent on z = (log E, nu / NU_SCALE): every mesh keeps its own 2x2
+    BFGS inverse-Hessian estimate and its own backtracking line search.  Each trial point of all
+    meshes is one batched forward + adjoint (loss and gradient of every mesh at once); a mesh whose
+    loss falls by the Armijo condition accepts its trial, the others halve their step and try again.
+    Steps are capped at max_step per coordinate and nu is kept inside nu_bounds.  Returns
+    (logE, nu, history of the total loss at the accepted points, per-mesh final losses)."""
+    M = len(problem.batch.meshes)
+    z = np.stack([np.asarray(logE0, np.float64), np.asarray(nu0, np.float64) / NU_SCALE], axis=1)
+    lo = np.array([-np.inf, nu_bounds[0] / NU_SCALE])
+    hi = np.array([np.inf, nu_bounds[1] / NU_SCALE])
+    cap = np.asarray(max_step, np.float64)
+
+    def evaluate(zz):
+        L, gE, gN = problem.loss_and_grad(zz[:, 0], zz[:, 1] * NU_SCALE, targets)
+        return L, np.stack([gE, gN * NU_SCALE], axis=1)
+
+    L, g = evaluate(z)
+    hist = [float(L.sum())]
+    Hinv = np.zeros((M, 2, 2))
+
+    def reset(m):
+        Hinv[m] = np.eye(2) * (0.5 / max(np.abs(g[m]).max(), 1e-300))
+
+    for m in range(M):
+        reset(m)
+    for _ in range(outer):
+        d = -np.einsum("mij,mj->mi", Hinv, g)
+        for m in range(M):
+            if g[m] @ d[m] >= 0.0:  # not a descent direction: restart from a scaled gradient step
+                reset(m)
+                d[m] = -Hinv[m] @ g[m]
+        d *= np.minimum(1.0, np.min(cap / np.maximum(np.abs(d), 1e-300), axis=1))[:, None]
+        alpha = np.ones(M)
+        done = np.zeros(M, bool)
+        z_new, L_new, g_new = z.copy(), L.copy(), g.copy()
+        for _ in range(tries):
+            trial = np.where(done[:, None], z_new, np.clip(z + alpha[:, None] * d, lo, hi))
+            Lt, gt = evaluate(trial)
+            step = trial - z
+            ok = ~done & (Lt <= L + armijo * np.einsum("mi,mi->m", g, step))
+            z_new[ok], L_new[ok], g_new[ok] = trial[ok], Lt[ok], gt[ok]
+            done |= ok
+            if done.all():
+                break
+            alpha[~done] *= 0.5
+        for m in range(M):
+            s_ = z_new[m] - z[m]
+            y_ = g_new[m] - g[m]
+            sy = float(s_ @ y_)
+            if not done[m]:
+                continue
+            if sy > 1e-12 * np.linalg.norm(s_) * np.linalg.norm(y_):
+                rho = 1.0 / sy
+                V = np.eye(2) - rho * np.outer(s_, y_)
+                Hinv[m] = V @ Hinv[m] @ V.T + rho * np.outer(s_, s_)
+        z, L, g = z_new, L_new, g_new
+        for m in np.flatnonzero(~done):
+            reset(m)
+        hist.append(float(L.sum()))
+    return z[:, 0], z[:, 1] * NU_SCALE, hist, L
+
+
+def identify_adam(problem, targets, logE0, nu0, outer=50, lr_logE=0.15, lr_nu=0.01, nu_bounds=(0.05, 0.48)):
     """Adam on per-mesh (log E, nu); returns (logE, nu, history of total loss)."""
     logE = np.array(logE0, np.float64)
     nu = np.array(nu0, np.float64)

@@ -208,6 +208,14 @@ class GPUSolver:
         call("vbd_solver_energy", self._h, int(kind), float(h), C.byref(out))
         return out.value
 
+    def energy_history(self, reset: bool = True) -> np.ndarray:
+        """The energies vbd_solver_step appended under OPT_ENERGY_EVERY (oldest first)."""
+        n = C.c_int32(0)
+        call("vbd_solver_energy_history", self._h, None, 0, C.byref(n), 0)
+        out = np.empty(n.value, np.float64)
+        call("vbd_solver_energy_history", self._h, _ptr(out), n.value, C.byref(n), int(bool(reset)))
+        return out
+
     def status(self, reset: bool = False):
         sing = C.c_int64(0)
         nonf = C.c_int32(0)
@@ -222,6 +230,21 @@ class GPUSolver:
         call("vbd_solver_get_option", self._h, int(option), C.byref(v))
         return v.value
 
+    def set_colour_lanes(self, lanes=None) -> None:
+        """Threads per vertex for each colour (None: VBD_OPT_LANES for every colour)."""
+        if lanes is None:
+            call("vbd_solver_set_colour_lanes", self._h, 0, None)
+            return
+        arr = _i32(lanes)
+        call("vbd_solver_set_colour_lanes", self._h, int(arr.shape[0]), _ptr(arr))
+
+    def get_colour_lanes(self) -> np.ndarray:
+        nc = C.c_int32(0)
+        call("vbd_solver_info", self._h, None, None, C.byref(nc))
+        out = np.empty(nc.value, np.int32)
+        call("vbd_solver_get_colour_lanes", self._h, nc.value, _ptr(out))
+        return out
+
     def kernel_time(self, reset: bool = False):
         """(summed sweep-kernel ms, sweep launches, algorithmic bytes) timed since the last reset."""
         ms = C.c_double(0.0)
@@ -231,10 +254,14 @@ class GPUSolver:
         return ms.value, n.value, b.value
 
     def autotune(self, dt: float, iterations: int = 10, repeats: int = 2) -> dict:
-        """Times the candidate launch shapes, keeps the fastest and restores the state."""
+        """Times the candidate launch configurations, keeps the fastest and restores the state."""
         out = (C.c_int32 * 5)()
         call("vbd_solver_autotune", self._h, float(dt), int(iterations), int(repeats), C.cast(out, C.c_void_p))
-        return dict(zip(("lanes", "layout", "prefetch", "pdl", "block"), list(out)))
+        res = dict(zip(("lanes", "layout", "prefetch", "pdl", "block"), list(out)))
+        res["record_cache"] = self.get_option(_capi.OPT_RECORD_CACHE)
+        res["persistent"] = self.get_option(_capi.OPT_PERSISTENT)
+        res["colour_lanes"] = self.get_colour_lanes().tolist()
+        return res
 
     def kernel_launches(self) -> int:
         v = C.c_int64(0)
