@@ -418,6 +418,7 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
         launches_b = (bs.kernel_launches() - l0) // (K + 1)
         xb = bs.get_positions()
         batch_lanes = bs.get_option(_capi.OPT_LANES)
+        batch_layout = bs.get_option(_capi.OPT_LAYOUT)
         # algorithmic bytes of one step's colour sweeps (60 B per incidence + 96 B per swept vertex),
         # from a pass with an event pair around every sweep (after the positions were read)
         bs.set_option(_capi.OPT_KERNEL_TIMING, 1)
@@ -426,9 +427,10 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
         bs.step(dt, iters, g, True, rho)
         sw_ms, sw_launches, sw_bytes = bs.kernel_time(reset=True)
         bs.close()
-        # the per-mesh solvers use the batch solver's lane count, so each mesh's arithmetic (and
-        # result) is the batch's
-        plain = [build_solver(m, device=local, stream=stream.cuda_stream, lanes=batch_lanes) for m in sub]
+        # the per-mesh solvers use the batch solver's lane count and record layout, so each mesh's
+        # arithmetic (and result) is the batch's
+        plain = [build_solver(m, device=local, stream=stream.cuda_stream, lanes=batch_lanes, layout=batch_layout)
+                 for m in sub]
         l0 = sum(p.kernel_launches() for p in plain)
 
         def plain_step():
@@ -484,6 +486,8 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
         "launches_per_step": int(launches_b),
         "plain_launches_per_step": int(launches_p),
         "bitwise_equal_to_plain": mism == 0.0,
+        "lanes": int(batch_lanes),
+        "layout": int(batch_layout),
         "sharding": f"whole meshes over {world} rank(s), balanced by tet count" if world > 1 else "single GPU",
         "roofline": roofline,
     }

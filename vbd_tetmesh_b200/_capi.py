@@ -59,6 +59,7 @@ SIGNATURES = {
     "vbd_color_vertices": [_i32, _i32, _p, _p, _PI32, _i32, _p, _p],
     "vbd_mesh_mass": [_i32, _i32, _p, _p, _f32, _p, _p],
     "vbd_precompute_tets": [_i32, _i32, _p, _p, _p, _p],
+    "vbd_factored_record_error": [_i32, _p, _PF64, _PF64, _PF64],
     "vbd_tetgen_read_node": [C.c_char_p, _PI32, _PI32, _p, _i32],
     "vbd_tetgen_read_ele": [C.c_char_p, _i32, _i32, _PI32, _p, _i32],
     "vbd_pin_low_fraction": [_i32, _p, _i32, _f32, _p],

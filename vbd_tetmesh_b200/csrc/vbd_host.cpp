@@ -1,5 +1,6 @@
 // Host-side mesh set-up of libvbd_b200: greedy vertex colouring, lumped masses, rest-shape
 // inverses.  Pure integer / FP32 host work, run once per mesh; no GPU needed.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -53,9 +54,86 @@ void build_vertex_tets(int32_t num_verts, int32_t num_tets, const int32_t* tets,
         for (int a = 0; a < 4; ++a) tet_ids[fill[tets[4 * t + a]]++] = t;
 }
 
+// Largest relative error, over every tet and local vertex n, of det M as the factored record
+// layouts obtain it in FP32, against det M in FP64 of the same FP32 rows.  M is the 3x3 matrix of
+// the other three rows q_k of Q = Ps Dm^-1 and q_n = -(q_a + q_b + q_c).  Layout 3 stores det M =
+// M_0 . cof(M)_0; layout 4 derives it as s.w / |q_n|^2 with s = M q_n, w = cof(M) q_n and |q_n|^2 =
+// -(s_0 + s_1 + s_2), which cancels when |q_n| is small next to the other rows (anisotropic or
+// sliver tets).  The FP32 steps follow k_pack_factored and decode_fact.
+void factored_detm_error(int32_t num_tets, const float* dm_inv, double* err3, double* err4, double* excess4) {
+    double e3 = 0.0, e4 = 0.0, x4 = 0.0;
+    for (int64_t t = 0; t < num_tets; ++t) {
+        const float* d = dm_inv + 9 * t;
+        float Q[4][3];
+        for (int c = 0; c < 3; ++c) {
+            Q[0][c] = -d[c] - d[3 + c] - d[6 + c];
+            for (int k = 1; k < 4; ++k) Q[k][c] = d[3 * (k - 1) + c];
+        }
+        for (int n = 0; n < 4; ++n) {
+            float M[3][3];
+            int m = 0;
+            for (int k = 0; k < 4; ++k) {
+                if (k == n) continue;
+                for (int c = 0; c < 3; ++c) M[m][c] = Q[k][c];
+                ++m;
+            }
+            const float q[3] = {-(M[0][0] + M[1][0] + M[2][0]), -(M[0][1] + M[1][1] + M[2][1]),
+                                -(M[0][2] + M[1][2] + M[2][2])};
+            float cof[3][3];
+            for (int i = 0; i < 3; ++i) {
+                const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+                for (int c = 0; c < 3; ++c) {
+                    const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+                    cof[i][c] = M[i1][c1] * M[i2][c2] - M[i1][c2] * M[i2][c1];
+                }
+            }
+            float sv[3], wv[3];
+            for (int i = 0; i < 3; ++i) {
+                sv[i] = M[i][0] * q[0] + M[i][1] * q[1] + M[i][2] * q[2];
+                wv[i] = cof[i][0] * q[0] + cof[i][1] * q[1] + cof[i][2] * q[2];
+            }
+            const float det3 = M[0][0] * cof[0][0] + M[0][1] * cof[0][1] + M[0][2] * cof[0][2];
+            const float qq = -(sv[0] + sv[1] + sv[2]);
+            const float sw = std::fma(sv[2], wv[2], std::fma(sv[1], wv[1], sv[0] * wv[0]));
+            const float det4 = sw / qq;
+            double Md[3][3];
+            for (int i = 0; i < 3; ++i)
+                for (int c = 0; c < 3; ++c) Md[i][c] = M[i][c];
+            const double exact = Md[0][0] * (Md[1][1] * Md[2][2] - Md[1][2] * Md[2][1]) -
+                                 Md[0][1] * (Md[1][0] * Md[2][2] - Md[1][2] * Md[2][0]) +
+                                 Md[0][2] * (Md[1][0] * Md[2][1] - Md[1][1] * Md[2][0]);
+            if (exact == 0.0 || !std::isfinite(exact)) {
+                e3 = e4 = x4 = INFINITY;
+                continue;
+            }
+            const double r3 = std::fabs((double)det3 / exact - 1.0), r4 = std::fabs((double)det4 / exact - 1.0);
+            e3 = std::isfinite(r3) ? std::max(e3, r3) : INFINITY;
+            e4 = std::isfinite(r4) ? std::max(e4, r4) : INFINITY;
+            // layout 4's error against what this incidence allows it: the tolerance, or a few times
+            // the stored det M's own error (the conditioning of Dm^-1).  Tets that are degenerate in
+            // FP32 (the stored det M already off by more than kFactoredDegenerate) give no usable
+            // element in any FP32 form and are left out.
+            if (std::isfinite(r3) && r3 > kFactoredDegenerate) continue;
+            const double allowed = std::max(kFactoredDetmTol, kFactoredDetmRatio * r3);
+            x4 = std::isfinite(r4) && std::isfinite(allowed) ? std::max(x4, r4 / allowed) : INFINITY;
+        }
+    }
+    if (err3) *err3 = e3;
+    if (err4) *err4 = e4;
+    if (excess4) *excess4 = x4;
+}
+
 }  // namespace vbd
 
 extern "C" {
+
+int vbd_factored_record_error(int32_t num_tets, const float* dm_inv, double* err_layout3, double* err_layout4,
+                              double* layout4_excess) {
+    vbd::clear_error();
+    if (num_tets < 0 || (num_tets > 0 && !dm_inv)) VBD_FAIL(VBD_ERR_INVALID_ARG, "need dm_inv[9 * num_tets]");
+    vbd::factored_detm_error(num_tets, dm_inv, err_layout3, err_layout4, layout4_excess);
+    return VBD_OK;
+}
 
 int vbd_version(void) { return 100; }
 

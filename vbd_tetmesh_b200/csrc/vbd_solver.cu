@@ -1001,7 +1001,16 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
         while (L < 16 && largest * L * 2 <= (long long)sms * 1024) L *= 2;
         s->lanes = L;
     }
-    if (s->layout_auto) s->layout = N <= vbd::kPackedMaxVertices ? 4 : 3;
+    if (s->layout_auto) {
+        // Layout 4 derives det M from s and w, which cancels on anisotropic tets (a vertex whose row
+        // of Ps Dm^-1 is small next to the others); layout 3 stores det M.  On sliver tets both carry
+        // the FP32 conditioning error of Dm^-1 itself, which the reference's own F = Ds Dm^-1 shares.
+        // So layout 4 is kept unless, on some incidence, its det M is worse than both the tolerance
+        // and a few times layout 3's.
+        double e3 = 0.0, e4 = 0.0, x4 = 0.0;
+        vbd::factored_detm_error(T, dm_inv, &e3, &e4, &x4);
+        s->layout = (N <= vbd::kPackedMaxVertices && x4 <= 1.0) ? 4 : 3;
+    }
     s->max_valence = 0;
     for (int i = 0; i < nfree; ++i) s->max_valence = std::max(s->max_valence, inc_off[i + 1] - inc_off[i]);
     s->colour_maxval.assign(num_colours, 0);

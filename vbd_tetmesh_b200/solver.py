@@ -66,6 +66,15 @@ def precompute_tets(rest: np.ndarray, tets: np.ndarray):
     return dminv, v0
 
 
+def factored_record_error(dm_inv: np.ndarray):
+    """(layout 3, layout 4) worst relative FP32 error of det M in the factored records, and layout 4's
+    worst error over what an incidence allows it (above 1: the automatic choice takes layout 3)."""
+    d = _f32(dm_inv, (-1, 9))
+    e3, e4, x4 = C.c_double(0.0), C.c_double(0.0), C.c_double(0.0)
+    call("vbd_factored_record_error", int(d.shape[0]), _ptr(d), C.byref(e3), C.byref(e4), C.byref(x4))
+    return e3.value, e4.value, x4.value
+
+
 class GPUSolver:
     """One mesh (or batch of meshes) resident on one B200; wraps a ``vbd_solver*`` handle.
 
