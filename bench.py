@@ -60,6 +60,8 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-meshes", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=3)
+    ap.add_argument("--no-plain", action="store_true",
+                    help="batched section without the per-mesh solvers it is compared with (for profiling)")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-material-id", action="store_true")
     ap.add_argument("--clocks-dir", default=None,
@@ -429,19 +431,22 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
         bs.close()
         # the per-mesh solvers use the batch solver's lane count and record layout, so each mesh's
         # arithmetic (and result) is the batch's
-        plain = [build_solver(m, device=local, stream=stream.cuda_stream, lanes=batch_lanes, layout=batch_layout)
-                 for m in sub]
-        l0 = sum(p.kernel_launches() for p in plain)
+        if args.no_plain:
+            ms_p, launches_p, xp = float("nan"), 0, xb
+        else:
+            plain = [build_solver(m, device=local, stream=stream.cuda_stream, lanes=batch_lanes, layout=batch_layout)
+                     for m in sub]
+            l0 = sum(p.kernel_launches() for p in plain)
 
-        def plain_step():
+            def plain_step():
+                for p in plain:
+                    p.step(dt, iters, g, True, rho)
+
+            ms_p = timed(plain_step)
+            launches_p = (sum(p.kernel_launches() for p in plain) - l0) // (K + 1)
+            xp = np.concatenate([p.get_positions() for p in plain])
             for p in plain:
-                p.step(dt, iters, g, True, rho)
-
-        ms_p = timed(plain_step)
-        launches_p = (sum(p.kernel_launches() for p in plain) - l0) // (K + 1)
-        xp = np.concatenate([p.get_positions() for p in plain])
-        for p in plain:
-            p.close()
+                p.close()
     same = bool(np.array_equal(xb, xp))
     (ms_b, ms_p), (nverts, mism) = combine_over_ranks([ms_b, ms_p], [float(b.num_verts), 0.0 if same else 1.0],
                                                       dist, f"cuda:{local}")

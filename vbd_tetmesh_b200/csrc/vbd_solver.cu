@@ -73,10 +73,15 @@ using SweepFn = void (*)(SweepParams);
 // record loads with an L2 policy (factored layouts; k_sweep's CACHE).
 template <int L, int LAYOUT, bool CACHE> static SweepFn pick_depth(int prefetch) {
     if (prefetch == 0) return &k_sweep<L, LAYOUT, 0, CACHE>;
-    if (LAYOUT >= 3 && L > 1 && prefetch == 1) return &k_sweep_capped<L, LAYOUT, 1, CACHE>;
-    if (prefetch == 1 || LAYOUT < 3) return &k_sweep<L, LAYOUT, 1, CACHE>;
-    if (prefetch == 3 && L > 1) return &k_sweep_capped<L, LAYOUT, 2, CACHE>;
-    return &k_sweep<L, LAYOUT, (LAYOUT < 3 ? 1 : 3), CACHE>;
+    if constexpr (LAYOUT >= 3 && L > 1) {
+        if (prefetch == 1) return &k_sweep_capped<L, LAYOUT, 1, CACHE>;
+        if (prefetch == 3) return &k_sweep_capped<L, LAYOUT, 2, CACHE>;
+        return &k_sweep<L, LAYOUT, 3, CACHE>;
+    } else if constexpr (LAYOUT >= 3) {
+        return prefetch == 1 ? &k_sweep<L, LAYOUT, 1, CACHE> : &k_sweep<L, LAYOUT, 3, CACHE>;
+    } else {
+        return &k_sweep<L, LAYOUT, 1, CACHE>;
+    }
 }
 
 template <int L> static SweepFn pick_sweep(int layout, int prefetch, bool cache) {
