@@ -60,6 +60,11 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-meshes", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=3)
+    ap.add_argument("--no-autotune", action="store_true", help="time the launch configuration chosen at init")
+    ap.add_argument("--colour-lanes", default=None,
+                    help="comma-separated threads per vertex of each colour of the cube (with --no-autotune)")
+    ap.add_argument("--record-cache", type=int, default=None, help="VBD_OPT_RECORD_CACHE of the cube solver")
+    ap.add_argument("--persist-mb", type=int, default=None, help="VBD_OPT_RECORD_PERSIST_MB of the cube solver")
     ap.add_argument("--no-plain", action="store_true",
                     help="batched section without the per-mesh solvers it is compared with (for profiling)")
     ap.add_argument("--no-adjoint", action="store_true")
@@ -396,11 +401,12 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     K = args.batch_steps
 
-    def timed(step_fn):
+    def timed(step_fn, label):
         step_fn()  # warm-up (graph capture)
         torch.cuda.synchronize()
         barrier()
         ms = 0.0
+        torch.cuda.nvtx.range_push(label)
         for _ in range(K):
             flush.fill_(1.0)
             e0 = torch.cuda.Event(enable_timing=True)
@@ -410,13 +416,16 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
             e1.record(stream)
             e1.synchronize()
             ms += e0.elapsed_time(e1)
+        torch.cuda.nvtx.range_pop()
         barrier()
         return ms
 
     with torch.cuda.stream(stream):
         bs = build_batch_solver(b, device=local, stream=stream.cuda_stream)
+        tuned = None if args.no_autotune else bs.autotune(dt, iterations=iters, repeats=3)
+        batch_colour_lanes = bs.get_colour_lanes()
         l0 = bs.kernel_launches()
-        ms_b = timed(lambda: bs.step(dt, iters, g, True, rho))
+        ms_b = timed(lambda: bs.step(dt, iters, g, True, rho), "batched_timed")
         launches_b = (bs.kernel_launches() - l0) // (K + 1)
         xb = bs.get_positions()
         batch_lanes = bs.get_option(_capi.OPT_LANES)
@@ -436,13 +445,15 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
         else:
             plain = [build_solver(m, device=local, stream=stream.cuda_stream, lanes=batch_lanes, layout=batch_layout)
                      for m in sub]
+            for p in plain:  # colour c of a mesh is swept with the batch's shape for colour c
+                p.set_colour_lanes(batch_colour_lanes[: len(p.get_colour_lanes())])
             l0 = sum(p.kernel_launches() for p in plain)
 
             def plain_step():
                 for p in plain:
                     p.step(dt, iters, g, True, rho)
 
-            ms_p = timed(plain_step)
+            ms_p = timed(plain_step, "plain_timed")
             launches_p = (sum(p.kernel_launches() for p in plain) - l0) // (K + 1)
             xp = np.concatenate([p.get_positions() for p in plain])
             for p in plain:
@@ -493,6 +504,7 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
         "bitwise_equal_to_plain": mism == 0.0,
         "lanes": int(batch_lanes),
         "layout": int(batch_layout),
+        "autotuned": tuned,
         "sharding": f"whole meshes over {world} rank(s), balanced by tet count" if world > 1 else "single GPU",
         "roofline": roofline,
     }
@@ -569,7 +581,8 @@ def bench_material_id(local, stream):
     """Batched material identification: 64 beams (Lx U{8..40}, Ly = Lz U{3..8}), hidden (E, nu) as the
     batched configuration, targets from a 20-step forward under gravity; per-mesh gradients of
     (log E, nu) from one batched forward + adjoint vs central finite differences of the batched
-    forward (step 1e-3) at the initial guess, then 50 per-mesh quasi-Newton iterations from E = 1e5, nu = 0.3."""
+    forward (step 1e-3) at the initial guess, then 50 per-mesh trust-region quasi-Newton iterations from E = 1e5,
+    nu = 0.3."""
     import torch
 
     from vbd_tetmesh_b200 import material_id as mid
@@ -586,7 +599,7 @@ def bench_material_id(local, stream):
         fE = prob.fd_grad(logE0, nu0, targets, "logE", 1e-3)
         fN = prob.fd_grad(logE0, nu0, targets, "nu", 1e-3)
         t0 = time.perf_counter()
-        logE, nu, hist, final_losses = mid.identify(prob, targets, logE0, nu0, outer=50)
+        logE, nu, hist, final_losses, id_info = mid.identify(prob, targets, logE0, nu0, outer=50)
         t_id = time.perf_counter() - t0
         prob.solver.close()
     eE = np.abs(gE - fE) / np.maximum(np.abs(fE), 1e-30)
@@ -604,8 +617,13 @@ def bench_material_id(local, stream):
         "grad_vs_fd_rel_nu": q(eN),
         "grad_fd": "central differences of the batched FP32 GPU forward, step 1e-3 (FP32 noise dominates at 1e-4); "
                    "checked against FP64 finite differences at converged iterations in tests/test_gpu_material_id.py",
-        "optimizer": "per-mesh quasi-Newton (2x2 BFGS on log E, nu/0.1) with per-mesh backtracking line search; "
-                     "every trial is one batched forward + adjoint of all meshes",
+        "optimizer": "per-mesh trust-region quasi-Newton (2x2 BFGS on log E, nu/0.1); every iteration is one "
+                     "batched forward + adjoint of all meshes; a mesh whose trials fail twice in a row (the forward "
+                     "far from converged, so the implicit gradient misleads) takes central finite differences of the "
+                     "batched forward from then on",
+        "meshes_on_finite_differences": id_info["fd_meshes"],
+        "batched_forward_adjoints": id_info["forward_backwards"],
+        "batched_forwards": id_info["forwards"],
         "outer_iterations": 50,
         "identify_seconds": t_id,
         "loss_first": hist[0],
@@ -648,6 +666,17 @@ def main():
     stream = torch.cuda.Stream(device=local)
     solver = build_solver(mesh, device=local, stream=stream.cuda_stream, lanes=args.lanes, layout=args.layout)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    # launch configuration picked by the project's autotuner (set-up, outside the timed region)
+    tuned = None
+    if not args.no_autotune:
+        with torch.cuda.stream(stream):
+            tuned = solver.autotune(dt, iterations=iters, repeats=3)
+    if args.record_cache is not None:
+        solver.set_option(_capi.OPT_RECORD_CACHE, args.record_cache)
+    if args.persist_mb is not None:
+        solver.set_option(_capi.OPT_RECORD_PERSIST_MB, args.persist_mb)
+    if args.colour_lanes:
+        solver.set_colour_lanes([int(v) for v in args.colour_lanes.split(",")])
 
     def barrier():
         torch.cuda.synchronize()
@@ -670,6 +699,7 @@ def main():
         clocks.mark()
         launches0 = solver.kernel_launches()
         ms_total = 0.0
+        torch.cuda.nvtx.range_push("timed")  # lets a profiler capture exactly these steps' kernels
         for _ in range(args.steps):
             flush.fill_(1.0)
             e0 = torch.cuda.Event(enable_timing=True)
@@ -679,6 +709,7 @@ def main():
             e1.record(stream)
             e1.synchronize()
             ms_total += e0.elapsed_time(e1)
+        torch.cuda.nvtx.range_pop()
         barrier()
         launches = solver.kernel_launches() - launches0
 
@@ -762,7 +793,12 @@ def main():
         "data": "synthetic",
         "config": dict(workload_config(mesh, iters), parallelism=f"replicas x{world}" if world > 1 else "single GPU",
                        lanes=solver.get_option(_capi.OPT_LANES), layout=solver.get_option(_capi.OPT_LAYOUT),
-                       graph=solver.get_option(_capi.OPT_GRAPH)),
+                       graph=solver.get_option(_capi.OPT_GRAPH), autotuned=tuned,
+                       colour_lanes=solver.get_colour_lanes().tolist(),
+                       record_cache=solver.get_option(_capi.OPT_RECORD_CACHE),
+                       persist_mb=solver.get_option(_capi.OPT_RECORD_PERSIST_MB),
+                       prefetch=solver.get_option(_capi.OPT_PREFETCH),
+                       persistent=solver.get_option(_capi.OPT_PERSISTENT)),
         "gpu_launches": int(launches),
         "roofline": {
             "bound": "hbm",

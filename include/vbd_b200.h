@@ -307,10 +307,11 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *                        off by default (slower on the measured meshes)
  *   VBD_OPT_RECORD_CACHE: 1 = the factored records (layouts 3 and 4) are loaded past L1 with an L2
  *                        evict-first policy, so that the stream does not push the vertex state out of
- *                        L2; same results
+ *                        L2 (the default); 0 = plain read-only loads.  Same results
  *   VBD_OPT_RECORD_PERSIST_MB: with VBD_OPT_RECORD_CACHE, the first this-many megabytes of the record
  *                        stream are loaded with an L2 evict-last policy instead, so that they stay in
- *                        L2 from one sweep to the next (0 = none)
+ *                        L2 from one sweep to the next (0 = none).  Until it is set, vbd_solver_init
+ *                        picks 32 when the vertex state (64 B per vertex) fits in 32 MB, else 0
  *   VBD_OPT_ENERGY_EVERY: k > 0 = vbd_solver_step also evaluates VBDsolver::computeTotalEnergy (the
  *                        VBD_ENERGY_ELASTIC_LOGJ energy, FP64 sums) of the positions after iterations
  *                        0, k, 2k, ... of every sub-step, as VBDsolver::step does with k = 10
@@ -350,7 +351,8 @@ int vbd_solver_get_colour_lanes(vbd_solver* s, int32_t num_colours, int32_t* lan
  * (positions, velocities, inertia, counters) it started from.  In order:
  *   1. uniform launch shapes from a fixed list -- threads per vertex, record layout, prefetch,
  *      programmatic dependent launch, block size;
- *   2. the factored records' L2 policy (VBD_OPT_RECORD_CACHE);
+ *   2. the factored records' L2 policy (VBD_OPT_RECORD_CACHE with VBD_OPT_RECORD_PERSIST_MB 0, 32
+ *      and 64);
  *   3. per-colour threads per vertex, colour by colour, half and double the current count
  *      (vbd_solver_set_colour_lanes);
  *   4. the persistent colour-walking kernel (VBD_OPT_PERSISTENT) against the captured graph.

@@ -36,41 +36,58 @@ def test_batched_gradients_equal_per_mesh_gradients(gpu_device):
     prob.solver.close()
 
 
-def _oracle_loss(m, logE, nu, target, st):
-    """The FP64 oracle's forward of one beam from rest with (E, nu) on every tet, and its loss."""
-    E = np.exp(logE)
-    mu, lam, _, _ = mid.lame_and_derivatives(E, nu)
+def _oracle(m, logE, nu, st, dLdx=None):
+    """The FP64 oracle's forward of one beam from rest with (E, nu) on every tet, and, with dLdx,
+    its implicit adjoint (each step's (M/h^2 + H) lam = G solved by CG)."""
+    mu, lam, _, _ = mid.lame_and_derivatives(np.exp(logE), nu)
     T = m.num_tets
-    x = po.adjoint_f64(m, st.steps, st.dt, st.iterations, None, gravity=st.gravity, use_acceleration=True,
-                       rho=st.rho, x0=m.rest, v0=np.zeros_like(m.rest), mu=np.full(T, mu), lam=np.full(T, lam))["x"]
-    return float(np.sum((x - target) ** 2))
+    return po.adjoint_f64(m, st.steps, st.dt, st.iterations, dLdx, gravity=st.gravity, use_acceleration=True,
+                          rho=st.rho, x0=m.rest, v0=np.zeros_like(m.rest), mu=np.full(T, mu), lam=np.full(T, lam))
 
 
-def test_per_mesh_gradients_match_fp64_finite_differences(gpu_device):
-    """With every step's forward converged (200 iterations), the batched adjoint's per-mesh
-    d(loss)/d(log E) and d(loss)/d(nu) match central finite differences of the FP64 oracle's forward
-    of each mesh on its own (step 1e-4 in log E, 1e-4 nu in nu) within 1e-3, at a point away from
-    the hidden parameters."""
+def _oracle_loss(m, logE, nu, target, st):
+    return float(np.sum((_oracle(m, logE, nu, st)["x"] - target) ** 2))
+
+
+def test_per_mesh_gradients_match_fp64(gpu_device):
+    """The batched adjoint's per-mesh d(loss)/d(log E) and d(loss)/d(nu), at a point away from the
+    hidden parameters, against FP64 (6 steps of 200 iterations):
+    * on every mesh, against the FP64 implicit adjoint of the same steps, within 1e-3 (the quantity
+      the adjoint computes, with its sweeps run to convergence);
+    * against central finite differences of the FP64 forward (step 1e-4) within 1e-3 on the meshes
+      whose forward has converged at 200 iterations, i.e. where the finite differences of the
+      iteration map equal the implicit gradient within 1e-4.  A stiff, nearly incompressible beam
+      (E 8.9e5, nu 0.42) is still 60% away at 200 iterations and 1.7% at 800, so it takes part in
+      the first check only."""
     meshes, hidden = small_problem()
-    st = mid.Settings(steps=6, iterations=200, adjoint_iterations=150)
+    st = mid.Settings(steps=6, iterations=200, adjoint_iterations=1000)
     prob = mid.Problem.create(meshes, st)
     targets = prob.forward(np.log(hidden[:, 0]), hidden[:, 1])
     lE = np.log(hidden[:, 0]) + 0.4
     nu = hidden[:, 1] - 0.06
     _, gE, gN = prob.loss_and_grad(lE, nu, targets)
     prob.solver.close()
-    errs = []
+    converged = 0
     for k, m in enumerate(meshes):
         tk = targets[prob.batch.vert_offsets[k]:prob.batch.vert_offsets[k + 1]]
+        o = _oracle(m, lE[k], nu[k], st, lambda x: 2.0 * (x - tk))
+        mu, lam, dmu, dlam = mid.lame_and_derivatives(np.exp(lE[k]), nu[k])
+        iE = float(np.sum(o["gmu"] * mu + o["glam"] * lam))
+        iN = float(np.sum(o["gmu"] * dmu + o["glam"] * dlam))
         h = 1e-4
         fE = (_oracle_loss(m, lE[k] + h, nu[k], tk, st) - _oracle_loss(m, lE[k] - h, nu[k], tk, st)) / (2 * h)
         hn = 1e-4 * nu[k]
         fN = (_oracle_loss(m, lE[k], nu[k] + hn, tk, st) - _oracle_loss(m, lE[k], nu[k] - hn, tk, st)) / (2 * hn)
-        eE, eN = abs(gE[k] - fE) / abs(fE), abs(gN[k] - fN) / abs(fN)
-        print(f"mesh {k} dims {m.dims}: dL/dlogE adjoint {gE[k]:.6e} fd64 {fE:.6e} rel {eE:.2e}; "
-              f"dL/dnu adjoint {gN[k]:.6e} fd64 {fN:.6e} rel {eN:.2e}")
-        errs += [eE, eN]
-    assert max(errs) < GRAD_RTOL, errs
+        rel = lambda a, b: abs(a - b) / abs(b)  # noqa: E731
+        conv = rel(iE, fE) < 1e-4 and rel(iN, fN) < 1e-4
+        print(f"mesh {k} dims {m.dims}: dL/dlogE adjoint {gE[k]:.6e} implicit64 {iE:.6e} ({rel(gE[k], iE):.1e}) "
+              f"fd64 {fE:.6e} ({rel(gE[k], fE):.1e}); dL/dnu adjoint {gN[k]:.6e} implicit64 {iN:.6e} "
+              f"({rel(gN[k], iN):.1e}) fd64 {fN:.6e} ({rel(gN[k], fN):.1e}); forward converged: {conv}")
+        assert rel(gE[k], iE) < GRAD_RTOL and rel(gN[k], iN) < GRAD_RTOL
+        if conv:
+            converged += 1
+            assert rel(gE[k], fE) < GRAD_RTOL and rel(gN[k], fN) < GRAD_RTOL
+    assert converged >= 3
 
 
 def test_identification_recovers_hidden_materials(gpu_device):
@@ -79,11 +96,11 @@ def test_identification_recovers_hidden_materials(gpu_device):
     targets = prob.forward(np.log(hidden[:, 0]), hidden[:, 1])
     lE0 = np.full(len(meshes), np.log(1e5))
     nu0 = np.full(len(meshes), 0.3)
-    logE, nu, hist, final = mid.identify(prob, targets, lE0, nu0, outer=30)
+    logE, nu, hist, final, info = mid.identify(prob, targets, lE0, nu0, outer=30)
     prob.solver.close()
     relE = np.abs(np.exp(logE) / hidden[:, 0] - 1.0)
     dnu = np.abs(nu - hidden[:, 1])
-    print(f"loss {hist[0]:.4e} -> {hist[-1]:.4e}; E rel err {relE}, nu abs err {dnu}, final losses {final}")
+    print(f"loss {hist[0]:.4e} -> {hist[-1]:.4e}; E rel err {relE}, nu abs err {dnu}, final losses {final}, {info}")
     assert hist[-1] < 1e-3 * hist[0]
     assert np.all(np.diff(hist) <= 0.0)  # every accepted step lowers the loss
     assert relE.max() < 0.05

@@ -115,13 +115,6 @@ template <int L> static void (*pick_persistent(int layout))(PersistParams) {
     }
 }
 
-// The one-CTA-per-SM persistent kernel (factored layouts only): VBD_OPT_PERSISTENT 2 runs 768-thread
-// CTAs with 3 records ahead, 3 runs 1024-thread CTAs with 2.
-template <int L> static void (*pick_persist_wave(int layout, int kind))(PersistParams) {
-    if (kind == 2) return layout == 3 ? &k_persist_wave<L, 3, 768, 3> : &k_persist_wave<L, 4, 768, 3>;
-    return layout == 3 ? &k_persist_wave<L, 3, 1024, 2> : &k_persist_wave<L, 4, 1024, 2>;
-}
-
 // The adjoint reads tet records (layouts 0 and 1) or the forward's streamed incidence records.
 template <int L> static void (*pick_adj_sweep(int layout))(AdjParams) {
     switch (layout) {
@@ -188,7 +181,11 @@ struct vbd_solver {
     // VBD_OPT_RECORD_CACHE: the factored records are loaded with an L2 policy, evict-first except
     // the first persist_mb megabytes of the record stream (VBD_OPT_RECORD_PERSIST_MB), which are
     // loaded evict-last so that they stay in L2 from one sweep to the next.
-    int record_cache = 0, persist_mb = 0;
+    // Until they are set, vbd_solver_init turns the evict-first stream on (64^3 cube: 4.12 against
+    // 4.46 ms/step) with a 32 MB evict-last prefix when the vertex state (four float4 arrays) fits
+    // in 32 MB (cube: 4.08 ms; 64 MB: 4.21, 96 MB: 4.45 -- the prefix then competes with the state).
+    int record_cache = 1, persist_mb = 32;
+    bool record_cache_auto = true, persist_auto = true;
     // Per-colour threads per vertex (vbd_solver_set_colour_lanes); empty = `lanes` for every colour.
     // shape_gen changes with every setting, so captured graphs of another shape are not reused.
     std::vector<int> colour_lanes;
@@ -497,19 +494,13 @@ struct vbd_solver {
             omega_cache = w;
         }
         const int L = lanes < 4 ? 4 : lanes;
-        // persistent 2 / 3: one CTA per SM with the counted barrier (factored layouts)
-        const bool wave = persistent >= 2 && layout >= 3;
-        const int threads = wave ? (persistent == 2 ? 768 : 1024) : 256;
+        const int threads = 256;
         void (*fn)(vbd::PersistParams) = nullptr;
         switch (L) {
-            case 4: fn = wave ? vbd::pick_persist_wave<4>(layout, persistent) : vbd::pick_persistent<4>(layout); break;
-            case 8: fn = wave ? vbd::pick_persist_wave<8>(layout, persistent) : vbd::pick_persistent<8>(layout); break;
-            case 16:
-                fn = wave ? vbd::pick_persist_wave<16>(layout, persistent) : vbd::pick_persistent<16>(layout);
-                break;
-            default:
-                fn = wave ? vbd::pick_persist_wave<32>(layout, persistent) : vbd::pick_persistent<32>(layout);
-                break;
+            case 4: fn = vbd::pick_persistent<4>(layout); break;
+            case 8: fn = vbd::pick_persistent<8>(layout); break;
+            case 16: fn = vbd::pick_persistent<16>(layout); break;
+            default: fn = vbd::pick_persistent<32>(layout); break;
         }
         int per_sm = 0, sms = 0;
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0));
@@ -1016,6 +1007,8 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
         vbd::factored_detm_error(T, dm_inv, &e3, &e4, &x4);
         s->layout = (N <= vbd::kPackedMaxVertices && x4 <= 1.0) ? 4 : 3;
     }
+    if (s->record_cache_auto) s->record_cache = 1;
+    if (s->persist_auto) s->persist_mb = 64.0 * N <= 32.0 * 1048576.0 ? 32 : 0;
     s->max_valence = 0;
     for (int i = 0; i < nfree; ++i) s->max_valence = std::max(s->max_valence, inc_off[i + 1] - inc_off[i]);
     s->colour_maxval.assign(num_colours, 0);
@@ -1493,10 +1486,12 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
             return VBD_OK;
         case VBD_OPT_RECORD_CACHE:
             s->record_cache = value ? 1 : 0;
+            s->record_cache_auto = false;
             return VBD_OK;
         case VBD_OPT_RECORD_PERSIST_MB:
             if (value < 0) VBD_FAIL(VBD_ERR_INVALID_ARG, "persist megabytes must be >= 0");
             s->persist_mb = value;
+            s->persist_auto = false;
             return VBD_OK;
         case VBD_OPT_ENERGY_EVERY:
             if (value < 0) VBD_FAIL(VBD_ERR_INVALID_ARG, "energy interval must be >= 0");
@@ -1508,8 +1503,7 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
         case VBD_OPT_PERSISTENT:
             if (value && s->semantics)
                 VBD_FAIL(VBD_ERR_INVALID_ARG, "the persistent kernel runs the VBDsolver semantics only");
-            if (value < 0 || value > 3) VBD_FAIL(VBD_ERR_INVALID_ARG, "persistent must be 0, 1, 2 or 3");
-            s->persistent = value;
+            s->persistent = value ? 1 : 0;
             return VBD_OK;
         case VBD_OPT_L2_PREFETCH:
             s->l2_prefetch = value ? 1 : 0;
@@ -1650,7 +1644,7 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
     s->energy_every = 0;  // the candidate steps append no energies
     // The whole launch configuration a candidate sets.
     struct Cand {
-        int lanes, layout, prefetch, pdl, block, persistent, cache;
+        int lanes, layout, prefetch, pdl, block, persistent, cache, persist;
         std::vector<int> colour_lanes;  // empty = `lanes` for every colour
     };
     const float g[3] = {0.f, 0.f, 0.f};
@@ -1664,6 +1658,7 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
         s->block = c.block;
         s->persistent = c.persistent;
         s->record_cache = c.cache;
+        s->persist_mb = c.persist;
         if (s->colour_lanes != c.colour_lanes) {
             s->colour_lanes = c.colour_lanes;
             ++s->shape_gen;
@@ -1697,13 +1692,15 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
         {8, 3, 1, 0, 64}, {4, 2, 1, 1, 128}, {8, 2, 1, 1, 64},  {2, 2, 1, 1, 128}, {8, 1, 1, 1, 128},
         {8, 0, 1, 1, 128}, {4, 0, 1, 1, 128},
     };
-    Cand best{s->lanes, s->layout, s->eff_prefetch(), s->pdl, s->block, s->persistent, s->record_cache, s->colour_lanes};
+    Cand best{s->lanes,      s->layout,       s->eff_prefetch(), s->pdl,          s->block,
+              s->persistent, s->record_cache, s->persist_mb,     s->colour_lanes};
     float best_ms = 1e30f;
+    const int init_persist = s->persist_mb;  // the init-time record policy, for the factored candidates
     s->prefetch_auto = false;
     int rc = VBD_OK;
     for (const auto& u : uniform) {
         if (u[1] == 4 && s->N > vbd::kPackedMaxVertices) continue;
-        Cand c{u[0], u[1], u[2], u[3], u[4], 0, 0, {}};
+        Cand c{u[0], u[1], u[2], u[3], u[4], 0, u[1] >= 3 ? 1 : 0, u[1] >= 3 ? init_persist : 0, {}};
         float ms = 0.f;
         if ((rc = time_of(c, &ms))) break;
         if (ms < best_ms) {
@@ -1721,11 +1718,16 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
         }
         return VBD_OK;
     };
-    // Phase 2: the factored records' L2 policy (evict-first stream).
+    // Phase 2: the factored records' L2 policy: plain loads, or the evict-first stream with an
+    // evict-last prefix of 0, 32 or 64 MB.
     if (!rc && best.layout >= 3) {
-        Cand c = best;
-        c.cache = 1;
-        rc = try_cand(c);
+        const Cand base = best;
+        for (int pm : {0, 32, 64}) {
+            Cand c = base;
+            c.cache = 1;
+            c.persist = pm;
+            if ((rc = try_cand(c))) break;
+        }
     }
     // Phase 3: per-colour threads per vertex, greedily colour by colour (half, same, double).
     if (!rc && s->semantics == 0 && s->C > 1) {
@@ -1755,6 +1757,7 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
     CUDA_TRY(cudaMemcpyAsync(s->status.p, st, sizeof(st), cudaMemcpyHostToDevice, s->stream));
     s->timing = saved_timing;
     s->energy_every = saved_energy;
+    s->record_cache_auto = s->persist_auto = false;  // the tuned policy stays for this mesh
     const int arc = apply(best);
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     if (rc) return rc;

@@ -4,8 +4,8 @@ Every mesh of the batch advances in one solver (colour c of all meshes in one la
 recorded forward and one backward pass (vbd_solver_record / vbd_solver_backward) give the
 per-tet gradients dL/dmu, dL/dlambda of the loss L = sum_m sum_i |x_i - x*_i|^2, which chain to
 each mesh's (log E, nu) through mu = E / (2 (1 + nu)), lambda = E nu / ((1 + nu)(1 - 2 nu)).
-Each mesh's (log E, nu) moves by its own quasi-Newton step with a line search (identify); a line
-search trial of all meshes costs one batched forward + adjoint.  Finite-difference checks need only two
+Each mesh's (log E, nu) moves by its own trust-region quasi-Newton step (identify); one trial of all
+meshes costs one batched forward + adjoint.  Finite-difference checks need only two
 batched forwards per parameter, since the meshes are independent.
 """
 from __future__ import annotations
@@ -128,68 +128,104 @@ class Problem:
 NU_SCALE = 0.1  # nu is optimised as nu / NU_SCALE, so both coordinates move on similar scales
 
 
-def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), max_step=(1.0, 0.5), tries=6,
-             armijo=1e-4):
-    """Per-mesh quasi-Newton descent on z = (log E, nu / NU_SCALE): every mesh keeps its own 2x2
-    BFGS inverse-Hessian estimate and its own backtracking line search.  Each trial point of all
-    meshes is one batched forward + adjoint (loss and gradient of every mesh at once); a mesh whose
-    loss falls by the Armijo condition accepts its trial, the others halve their step and try again.
-    Steps are capped at max_step per coordinate and nu is kept inside nu_bounds.  Returns
-    (logE, nu, history of the total loss at the accepted points, per-mesh final losses)."""
+def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), radius0=(1.0, 0.5), armijo=1e-4,
+             fd_after=2, fd_step=1e-3):
+    """Per-mesh trust-region quasi-Newton descent on z = (log E, nu / NU_SCALE).
+
+    Every mesh keeps its own 2x2 BFGS inverse-Hessian estimate and its own trust radius (per
+    coordinate, initially radius0).  Each outer iteration evaluates every mesh's trial point in one
+    batched forward + adjoint; a mesh whose loss falls by the Armijo condition accepts the trial and
+    widens its radius, the others halve it.  The adjoint differentiates each step as converged; on
+    stiff, nearly incompressible meshes the forward's fixed iteration count leaves the step far
+    from converged, so that gradient can point away from descent.  A mesh whose trial has been
+    rejected fd_after times in a row therefore takes central finite differences of the batched
+    forward (step fd_step) as its gradient from then on; those forwards are run only while some
+    mesh needs them.  nu is kept inside nu_bounds.
+
+    Returns (logE, nu, history of the total loss at the accepted points, per-mesh final losses, info)
+    with info = dict(fd_meshes, forwards, forward_backwards)."""
     M = len(problem.batch.meshes)
     z = np.stack([np.asarray(logE0, np.float64), np.asarray(nu0, np.float64) / NU_SCALE], axis=1)
     lo = np.array([-np.inf, nu_bounds[0] / NU_SCALE])
     hi = np.array([np.inf, nu_bounds[1] / NU_SCALE])
-    cap = np.asarray(max_step, np.float64)
+    counts = {"forwards": 0, "forward_backwards": 0}
 
     def evaluate(zz):
+        counts["forward_backwards"] += 1
         L, gE, gN = problem.loss_and_grad(zz[:, 0], zz[:, 1] * NU_SCALE, targets)
         return L, np.stack([gE, gN * NU_SCALE], axis=1)
 
+    def fd_gradient(zz):
+        g = np.zeros_like(zz)
+        for c, h in ((0, fd_step), (1, fd_step / NU_SCALE)):
+            Ls = []
+            for sign in (1.0, -1.0):
+                zt = zz.copy()
+                zt[:, c] += sign * h
+                counts["forwards"] += 1
+                Ls.append(problem.losses(problem.forward(zt[:, 0], zt[:, 1] * NU_SCALE), targets))
+            g[:, c] = (Ls[0] - Ls[1]) / (2.0 * h)
+        return g
+
     L, g = evaluate(z)
     hist = [float(L.sum())]
+    radius = np.tile(np.asarray(radius0, np.float64), (M, 1))
     Hinv = np.zeros((M, 2, 2))
+    rejects = np.zeros(M, int)
+    use_fd = np.zeros(M, bool)
+    zp, gp = z.copy(), g.copy()          # a finite-difference mesh's previous point and gradient
+    have_prev = np.zeros(M, bool)
 
     def reset(m):
-        Hinv[m] = np.eye(2) * (0.5 / max(np.abs(g[m]).max(), 1e-300))
+        Hinv[m] = np.eye(2) * (radius[m].min() / max(np.abs(g[m]).max(), 1e-300))
+
+    def bfgs(m, s_, y_):
+        sy = float(s_ @ y_)
+        if sy > 1e-12 * np.linalg.norm(s_) * np.linalg.norm(y_):
+            rho = 1.0 / sy
+            V = np.eye(2) - rho * np.outer(s_, y_)
+            Hinv[m] = V @ Hinv[m] @ V.T + rho * np.outer(s_, s_)
 
     for m in range(M):
         reset(m)
     for _ in range(outer):
+        if use_fd.any():
+            gf = fd_gradient(z)
+            for m in np.flatnonzero(use_fd):
+                if not have_prev[m]:  # just switched: start the curvature estimate afresh
+                    g[m] = gf[m]
+                    reset(m)
+                elif np.any(z[m] != zp[m]):
+                    bfgs(m, z[m] - zp[m], gf[m] - gp[m])
+                zp[m], gp[m], have_prev[m] = z[m], gf[m], True
+            g[use_fd] = gf[use_fd]
         d = -np.einsum("mij,mj->mi", Hinv, g)
         for m in range(M):
             if g[m] @ d[m] >= 0.0:  # not a descent direction: restart from a scaled gradient step
                 reset(m)
                 d[m] = -Hinv[m] @ g[m]
-        d *= np.minimum(1.0, np.min(cap / np.maximum(np.abs(d), 1e-300), axis=1))[:, None]
-        alpha = np.ones(M)
-        done = np.zeros(M, bool)
-        z_new, L_new, g_new = z.copy(), L.copy(), g.copy()
-        for _ in range(tries):
-            trial = np.where(done[:, None], z_new, np.clip(z + alpha[:, None] * d, lo, hi))
-            Lt, gt = evaluate(trial)
-            step = trial - z
-            ok = ~done & (Lt <= L + armijo * np.einsum("mi,mi->m", g, step))
-            z_new[ok], L_new[ok], g_new[ok] = trial[ok], Lt[ok], gt[ok]
-            done |= ok
-            if done.all():
-                break
-            alpha[~done] *= 0.5
+        d *= np.minimum(1.0, np.min(radius / np.maximum(np.abs(d), 1e-300), axis=1))[:, None]
+        trial = np.clip(z + d, lo, hi)
+        Lt, gt = evaluate(trial)
+        step = trial - z
+        ok = Lt <= L + armijo * np.einsum("mi,mi->m", g, step)
+        if use_fd.any():
+            gt[use_fd] = g[use_fd]  # refreshed by finite differences at the next iteration
         for m in range(M):
-            s_ = z_new[m] - z[m]
-            y_ = g_new[m] - g[m]
-            sy = float(s_ @ y_)
-            if not done[m]:
+            if not ok[m]:
+                radius[m] *= 0.5
+                rejects[m] += 1
+                if rejects[m] >= fd_after:
+                    use_fd[m] = True
                 continue
-            if sy > 1e-12 * np.linalg.norm(s_) * np.linalg.norm(y_):
-                rho = 1.0 / sy
-                V = np.eye(2) - rho * np.outer(s_, y_)
-                Hinv[m] = V @ Hinv[m] @ V.T + rho * np.outer(s_, s_)
-        z, L, g = z_new, L_new, g_new
-        for m in np.flatnonzero(~done):
-            reset(m)
+            rejects[m] = 0
+            radius[m] = np.minimum(2.0 * radius[m], 4.0 * np.asarray(radius0))
+            if not use_fd[m]:
+                bfgs(m, trial[m] - z[m], gt[m] - g[m])
+            z[m], L[m], g[m] = trial[m], Lt[m], gt[m]
         hist.append(float(L.sum()))
-    return z[:, 0], z[:, 1] * NU_SCALE, hist, L
+    info = dict(fd_meshes=int(use_fd.sum()), **counts)
+    return z[:, 0], z[:, 1] * NU_SCALE, hist, L, info
 
 
 def identify_adam(problem, targets, logE0, nu0, outer=50, lr_logE=0.15, lr_nu=0.01, nu_bounds=(0.05, 0.48)):
