@@ -65,6 +65,7 @@ def parse_args():
                     help="comma-separated threads per vertex of each colour of the cube (with --no-autotune)")
     ap.add_argument("--record-cache", type=int, default=None, help="VBD_OPT_RECORD_CACHE of the cube solver")
     ap.add_argument("--persist-mb", type=int, default=None, help="VBD_OPT_RECORD_PERSIST_MB of the cube solver")
+    ap.add_argument("--prefetch", type=int, default=None, help="VBD_OPT_PREFETCH of the cube solver")
     ap.add_argument("--no-plain", action="store_true",
                     help="batched section without the per-mesh solvers it is compared with (for profiling)")
     ap.add_argument("--no-adjoint", action="store_true")
@@ -675,6 +676,8 @@ def main():
         solver.set_option(_capi.OPT_RECORD_CACHE, args.record_cache)
     if args.persist_mb is not None:
         solver.set_option(_capi.OPT_RECORD_PERSIST_MB, args.persist_mb)
+    if args.prefetch is not None:
+        solver.set_option(_capi.OPT_PREFETCH, args.prefetch)
     if args.colour_lanes:
         solver.set_colour_lanes([int(v) for v in args.colour_lanes.split(",")])
 

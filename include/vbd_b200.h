@@ -76,13 +76,13 @@ int vbd_precompute_tets(int32_t num_verts, int32_t num_tets, const float* rest_x
 /* Accuracy of the factored element records on a mesh (no reference counterpart; host only): the
  * largest relative error, over every tet and local vertex, of the FP32 det M that record layout 3
  * stores and that layout 4 derives as s.w / |q_n|^2, against FP64 (M = the other three rows of
- * Ps Dm^-1, dm_inv float[9T] row-major as for vbd_solver_init); and layout4_excess, the largest
- * ratio of layout 4's error to max(1e-5, 4 x layout 3's error) on the same incidence, leaving out
- * tets that are degenerate in FP32 (layout 3's error above 1e-3), where no FP32 form of the element
- * is accurate (above 1: vbd_solver_init's automatic choice takes layout 3).  Any output may be
- * null. */
+ * Ps Dm^-1, dm_inv float[9T] row-major as for vbd_solver_init); and layout4_loss_fraction, the
+ * fraction of incidences on which layout 4's error is above both 1e-5 and 4 x layout 3's error
+ * there, leaving out tets that are degenerate in FP32 (layout 3's error above 1e-3), where no FP32
+ * form of the element is accurate (above 1e-3: vbd_solver_init's automatic choice takes layout 3).
+ * Any output may be null. */
 int vbd_factored_record_error(int32_t num_tets, const float* dm_inv, double* err_layout3, double* err_layout4,
-                              double* layout4_excess);
+                              double* layout4_loss_fraction);
 
 /* ------------------------------------------------------------------------------------------
  * TetGen input and pinning (the reference driver's loadTetgenModel / readNodeFile and its
@@ -269,9 +269,9 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *                            each, s, w and the material products; det M = s.w / |q_n|^2 derived):
  *                            meshes of at most 2^21 vertices only (VBD_ERR_INVALID_ARG otherwise)
  *                        Until it is set, vbd_solver_init picks layout 4 when the mesh has at most
- *                        2^21 vertices and layout 4's FP32 det M is, on every incidence, within 1e-5
- *                        relative of FP64 or within 4 times layout 3's error on that incidence
- *                        (vbd_factored_record_error; anisotropic meshes fail it), else layout 3.
+ *                        2^21 vertices and layout 4's FP32 det M loses accuracy on at most 0.1% of
+ *                        the incidences (vbd_factored_record_error; systematically anisotropic
+ *                        meshes exceed it), else layout 3.
  *                        Defaults: 64-thread blocks, PDL, graphs; lanes, layout and prefetch
  *                        chosen by vbd_solver_init.
  *   VBD_OPT_GRAPH:       1 = replay a captured CUDA graph per step, 0 = direct launches

@@ -106,12 +106,13 @@ def _c4_oracle(meshes, k, st, precision):
     return _C4_ORACLE[key]
 
 
-@pytest.mark.parametrize("layout", [None, 4])
+@pytest.mark.parametrize("layout", [None, 3])
 def test_batched_512_sample_matches_fp64(gpu_device, layout):
     """All 512 meshes advance in one solver (one launch per colour); every sampled mesh's positions
     after 60 steps lie within 1e-5 of its diagonal of its own FP64 oracle run, and of the FP32 one.
-    Run with the record layout the solver picks (its det M accuracy check takes the stored-det
-    layout 3 for this batch's thin tets) and with the packed layout 4 forced."""
+    Run with the record layout the solver picks (packed layout 4: the batch's thin tets are
+    isolated) and with the stored-det layout 3 forced: the derived det M's extra error on those
+    tets does not move the positions measurably."""
     meshes = meshgen.batched_blocks(C4_MESHES)
     b = meshgen.concat(meshes)
     st = C4_SETTINGS

@@ -17,10 +17,10 @@ def _err(m):
 
 
 def _keeps_packed(m):
-    """vbd_solver_init's automatic choice: the packed layout 4 unless some incidence's derived det M
-    is worse than both 1e-5 and 4 times the stored one's error there."""
+    """vbd_solver_init's automatic choice: the packed layout 4 unless its derived det M is worse than
+    both 1e-5 and 4 times the stored one's error on more than 0.1% of the incidences."""
     dm, _ = precompute_tets(m.rest, m.tets)
-    return factored_record_error(dm)[2] <= 1.0
+    return factored_record_error(dm)[2] <= 1e-3
 
 
 def flattened(factor, seed=4):
@@ -46,18 +46,19 @@ def test_anisotropic_mesh_needs_the_stored_det():
 
 
 def test_sliver_tets_limit_both_factored_layouts():
-    """Near-sliver tets carry the FP32 conditioning error of Dm^-1 in both factored layouts.  The
-    batched configuration's +-0.25-cell jitter makes thin tets in many meshes, on which the derived
-    det M of layout 4 is well past the stored one's: the automatic choice takes layout 3 for such a
-    mesh (and for a batch holding one)."""
+    """Near-sliver tets carry the FP32 conditioning error of Dm^-1 in both factored layouts; on a
+    mesh made of them (+-0.49-cell jitter) layout 4 loses accuracy on enough incidences for the
+    automatic choice to take layout 3.  The batched configuration's +-0.25-cell jitter makes only
+    isolated thin tets (a few incidences in a hundred thousand), so that batch keeps layout 4: its
+    positions after 60 steps are as close to FP64 with layout 4 as with layout 3
+    (tests/test_gpu_parity_headline.py)."""
     m = meshgen.jittered_block(8, 8, 8, cell=0.05, jitter=0.49, seed=3)
     e3, e4 = _err(m)
     assert e3 > TOL and e4 > TOL
-    meshes = meshgen.batched_blocks(16)
-    keep = [_keeps_packed(m) for m in meshes]
-    assert any(keep) and not all(keep)
-    dm = np.concatenate([precompute_tets(m.rest, m.tets)[0] for m in meshes])
-    assert factored_record_error(dm)[2] > 1.0
+    assert not _keeps_packed(m)
+    dm = np.concatenate([precompute_tets(m.rest, m.tets)[0] for m in meshgen.batched_blocks(64)])
+    e3, e4, frac = factored_record_error(dm)
+    assert e4 > TOL and 0.0 < frac < 1e-4
 
 
 def test_error_matches_a_numpy_restatement():

@@ -60,8 +60,9 @@ void build_vertex_tets(int32_t num_verts, int32_t num_tets, const int32_t* tets,
 // M_0 . cof(M)_0; layout 4 derives it as s.w / |q_n|^2 with s = M q_n, w = cof(M) q_n and |q_n|^2 =
 // -(s_0 + s_1 + s_2), which cancels when |q_n| is small next to the other rows (anisotropic or
 // sliver tets).  The FP32 steps follow k_pack_factored and decode_fact.
-void factored_detm_error(int32_t num_tets, const float* dm_inv, double* err3, double* err4, double* excess4) {
-    double e3 = 0.0, e4 = 0.0, x4 = 0.0;
+void factored_detm_error(int32_t num_tets, const float* dm_inv, double* err3, double* err4, double* frac4) {
+    double e3 = 0.0, e4 = 0.0;
+    long long counted = 0, over = 0;
     for (int64_t t = 0; t < num_tets; ++t) {
         const float* d = dm_inv + 9 * t;
         float Q[4][3];
@@ -103,24 +104,24 @@ void factored_detm_error(int32_t num_tets, const float* dm_inv, double* err3, do
                                  Md[0][1] * (Md[1][0] * Md[2][2] - Md[1][2] * Md[2][0]) +
                                  Md[0][2] * (Md[1][0] * Md[2][1] - Md[1][1] * Md[2][0]);
             if (exact == 0.0 || !std::isfinite(exact)) {
-                e3 = e4 = x4 = INFINITY;
+                e3 = e4 = INFINITY;
                 continue;
             }
             const double r3 = std::fabs((double)det3 / exact - 1.0), r4 = std::fabs((double)det4 / exact - 1.0);
             e3 = std::isfinite(r3) ? std::max(e3, r3) : INFINITY;
             e4 = std::isfinite(r4) ? std::max(e4, r4) : INFINITY;
-            // layout 4's error against what this incidence allows it: the tolerance, or a few times
-            // the stored det M's own error (the conditioning of Dm^-1).  Tets that are degenerate in
-            // FP32 (the stored det M already off by more than kFactoredDegenerate) give no usable
-            // element in any FP32 form and are left out.
+            // Does layout 4 lose accuracy here: is its error above the tolerance and above a few
+            // times the stored det M's own error (the conditioning of Dm^-1)?  Tets that are
+            // degenerate in FP32 (the stored det M already off by more than kFactoredDegenerate)
+            // give no usable element in any FP32 form and are left out.
             if (std::isfinite(r3) && r3 > kFactoredDegenerate) continue;
-            const double allowed = std::max(kFactoredDetmTol, kFactoredDetmRatio * r3);
-            x4 = std::isfinite(r4) && std::isfinite(allowed) ? std::max(x4, r4 / allowed) : INFINITY;
+            ++counted;
+            if (!(r4 <= std::max(kFactoredDetmTol, kFactoredDetmRatio * r3))) ++over;
         }
     }
     if (err3) *err3 = e3;
     if (err4) *err4 = e4;
-    if (excess4) *excess4 = x4;
+    if (frac4) *frac4 = counted ? (double)over / (double)counted : 0.0;
 }
 
 }  // namespace vbd
@@ -128,10 +129,10 @@ void factored_detm_error(int32_t num_tets, const float* dm_inv, double* err3, do
 extern "C" {
 
 int vbd_factored_record_error(int32_t num_tets, const float* dm_inv, double* err_layout3, double* err_layout4,
-                              double* layout4_excess) {
+                              double* layout4_loss_fraction) {
     vbd::clear_error();
     if (num_tets < 0 || (num_tets > 0 && !dm_inv)) VBD_FAIL(VBD_ERR_INVALID_ARG, "need dm_inv[9 * num_tets]");
-    vbd::factored_detm_error(num_tets, dm_inv, err_layout3, err_layout4, layout4_excess);
+    vbd::factored_detm_error(num_tets, dm_inv, err_layout3, err_layout4, layout4_loss_fraction);
     return VBD_OK;
 }
 

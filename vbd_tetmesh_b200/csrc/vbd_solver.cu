@@ -1001,11 +1001,11 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
         // Layout 4 derives det M from s and w, which cancels on anisotropic tets (a vertex whose row
         // of Ps Dm^-1 is small next to the others); layout 3 stores det M.  On sliver tets both carry
         // the FP32 conditioning error of Dm^-1 itself, which the reference's own F = Ds Dm^-1 shares.
-        // So layout 4 is kept unless, on some incidence, its det M is worse than both the tolerance
-        // and a few times layout 3's.
-        double e3 = 0.0, e4 = 0.0, x4 = 0.0;
-        vbd::factored_detm_error(T, dm_inv, &e3, &e4, &x4);
-        s->layout = (N <= vbd::kPackedMaxVertices && x4 <= 1.0) ? 4 : 3;
+        // So layout 4 is kept unless it loses accuracy on more than a small fraction of the
+        // incidences.
+        double e3 = 0.0, e4 = 0.0, f4 = 0.0;
+        vbd::factored_detm_error(T, dm_inv, &e3, &e4, &f4);
+        s->layout = (N <= vbd::kPackedMaxVertices && f4 <= vbd::kFactoredLossFraction) ? 4 : 3;
     }
     if (s->record_cache_auto) s->record_cache = 1;
     if (s->persist_auto) s->persist_mb = 64.0 * N <= 32.0 * 1048576.0 ? 32 : 0;
@@ -1719,13 +1719,15 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
         return VBD_OK;
     };
     // Phase 2: the factored records' L2 policy: plain loads, or the evict-first stream with an
-    // evict-last prefix of 0, 32 or 64 MB.
+    // evict-last prefix of 0, 32 or 64 MB.  (The 64^3 cube is fastest with the stream and 32 MB;
+    // the 512-mesh batch, whose vertex state alone outgrows L2, with plain loads.)
     if (!rc && best.layout >= 3) {
         const Cand base = best;
-        for (int pm : {0, 32, 64}) {
+        for (int pm : {-1, 0, 32, 64}) {
             Cand c = base;
-            c.cache = 1;
-            c.persist = pm;
+            c.cache = pm < 0 ? 0 : 1;
+            c.persist = pm < 0 ? 0 : pm;
+            if (c.cache == base.cache && c.persist == base.persist) continue;
             if ((rc = try_cand(c))) break;
         }
     }

@@ -129,7 +129,7 @@ NU_SCALE = 0.1  # nu is optimised as nu / NU_SCALE, so both coordinates move on 
 
 
 def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), radius0=(1.0, 0.5), armijo=1e-4,
-             fd_after=2, fd_step=1e-3):
+             fd_after=2, fd_step=1e-3, converged=1e-7):
     """Per-mesh trust-region quasi-Newton descent on z = (log E, nu / NU_SCALE).
 
     Every mesh keeps its own 2x2 BFGS inverse-Hessian estimate and its own trust radius (per
@@ -138,9 +138,10 @@ def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), rad
     widens its radius, the others halve it.  The adjoint differentiates each step as converged; on
     stiff, nearly incompressible meshes the forward's fixed iteration count leaves the step far
     from converged, so that gradient can point away from descent.  A mesh whose trial has been
-    rejected fd_after times in a row therefore takes central finite differences of the batched
-    forward (step fd_step) as its gradient from then on; those forwards are run only while some
-    mesh needs them.  nu is kept inside nu_bounds.
+    rejected fd_after times in a row, while its loss is still above `converged` times its initial
+    loss (below that, rejections come from FP32 noise in the loss), therefore takes central finite
+    differences of the batched forward (step fd_step) as its gradient from then on; those forwards
+    are run only while some mesh needs them.  nu is kept inside nu_bounds.
 
     Returns (logE, nu, history of the total loss at the accepted points, per-mesh final losses, info)
     with info = dict(fd_meshes, forwards, forward_backwards)."""
@@ -168,6 +169,7 @@ def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), rad
         return g
 
     L, g = evaluate(z)
+    L0 = L.copy()
     hist = [float(L.sum())]
     radius = np.tile(np.asarray(radius0, np.float64), (M, 1))
     Hinv = np.zeros((M, 2, 2))
@@ -215,7 +217,7 @@ def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), rad
             if not ok[m]:
                 radius[m] *= 0.5
                 rejects[m] += 1
-                if rejects[m] >= fd_after:
+                if rejects[m] >= fd_after and L[m] > converged * L0[m]:
                     use_fd[m] = True
                 continue
             rejects[m] = 0

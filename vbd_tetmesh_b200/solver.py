@@ -67,8 +67,8 @@ def precompute_tets(rest: np.ndarray, tets: np.ndarray):
 
 
 def factored_record_error(dm_inv: np.ndarray):
-    """(layout 3, layout 4) worst relative FP32 error of det M in the factored records, and layout 4's
-    worst error over what an incidence allows it (above 1: the automatic choice takes layout 3)."""
+    """(layout 3, layout 4) worst relative FP32 error of det M in the factored records, and the fraction
+    of incidences on which layout 4 loses accuracy (above 1e-3: the automatic choice takes layout 3)."""
     d = _f32(dm_inv, (-1, 9))
     e3, e4, x4 = C.c_double(0.0), C.c_double(0.0), C.c_double(0.0)
     call("vbd_factored_record_error", int(d.shape[0]), _ptr(d), C.byref(e3), C.byref(e4), C.byref(x4))
