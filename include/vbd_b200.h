@@ -353,9 +353,10 @@ int vbd_solver_get_colour_lanes(vbd_solver* s, int32_t num_colours, int32_t* lan
  *      programmatic dependent launch, block size;
  *   2. the factored records' L2 policy (VBD_OPT_RECORD_CACHE with VBD_OPT_RECORD_PERSIST_MB 0, 32
  *      and 64);
- *   3. per-colour threads per vertex, colour by colour in two passes, half and double the current
- *      count (vbd_solver_set_colour_lanes; timed over 2 x repeats steps), then the record prefetch
- *      again with those lanes;
+ *   3. per-colour threads per vertex (vbd_solver_set_colour_lanes): greedy over the colours, lane
+ *      counts 2, 4, 8 and 16, two passes, restarted under each prefetch depth of the factored
+ *      layouts; each candidate is timed alternately with the incumbent (twice each, 2 x repeats
+ *      steps) against drift;
  *   4. the persistent colour-walking kernel (VBD_OPT_PERSISTENT) against the captured graph.
  * Phases 2-4 replace the choice only when faster by more than 1%.  chosen (may be null) receives 5
  * ints: lanes, layout, prefetch, pdl, block; the rest of the choice is read back with

@@ -129,7 +129,8 @@ template <int L> static void (*pick_adj_sweep(int layout))(AdjParams) {
 struct GraphKey {
     int kind;  // 0 = step, 1 = solve, 2 = single sweep
     int iters, accel, init, lanes, layout, prefetch, pdl, block, semantics, l2_prefetch, src;
-    int record_cache, persist_mb, shape_gen, energy_every;
+    int record_cache, persist_mb, energy_every, pad_;
+    unsigned long long colour_shape;  // hash of the per-colour lanes (0 = uniform) and the mesh
     float h, dtsr, hg[3], rho;
     bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
 };
@@ -187,7 +188,8 @@ struct vbd_solver {
     int record_cache = 1, persist_mb = 32;
     bool record_cache_auto = true, persist_auto = true;
     // Per-colour threads per vertex (vbd_solver_set_colour_lanes); empty = `lanes` for every colour.
-    // shape_gen changes with every setting, so captured graphs of another shape are not reused.
+    // Graph keys carry a hash of the per-colour lanes and of the mesh generation (shape_gen, bumped
+    // by every vbd_solver_init), so a shape set again reuses its captured graph.
     std::vector<int> colour_lanes;
     std::vector<int> colour_maxval;     // most incident tets of a free vertex, per colour
     int shape_gen = 0;
@@ -311,7 +313,9 @@ struct vbd_solver {
         key.l2_prefetch = l2_prefetch;
         key.record_cache = record_cache;
         key.persist_mb = persist_mb;
-        key.shape_gen = shape_gen;
+        unsigned long long h = 1469598103934665603ull ^ (unsigned long long)shape_gen;  // FNV-1a
+        for (int L : colour_lanes) h = (h ^ (unsigned long long)L) * 1099511628211ull;
+        key.colour_shape = colour_lanes.empty() ? (unsigned long long)shape_gen : h;
         key.energy_every = energy_every;
     }
 
@@ -1573,7 +1577,6 @@ int vbd_solver_set_colour_lanes(vbd_solver* s, int32_t num_colours, const int32_
     VBD_TRY(need_ready(s));
     if (!lanes) {
         s->colour_lanes.clear();
-        ++s->shape_gen;
         return VBD_OK;
     }
     if (num_colours != s->C) VBD_FAIL(VBD_ERR_INVALID_ARG, "need one lane count per colour (%d), got %d", s->C, num_colours);
@@ -1583,7 +1586,6 @@ int vbd_solver_set_colour_lanes(vbd_solver* s, int32_t num_colours, const int32_
             VBD_FAIL(VBD_ERR_INVALID_ARG, "colour %d: lanes must be 1, 2, 4, 8, 16 or 32 (got %d)", c, v);
     }
     s->colour_lanes.assign(lanes, lanes + num_colours);
-    ++s->shape_gen;
     return VBD_OK;
 }
 
@@ -1659,10 +1661,7 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
         s->persistent = c.persistent;
         s->record_cache = c.cache;
         s->persist_mb = c.persist;
-        if (s->colour_lanes != c.colour_lanes) {
-            s->colour_lanes = c.colour_lanes;
-            ++s->shape_gen;
-        }
+        s->colour_lanes = c.colour_lanes;
         if (s->layout != c.layout) {
             s->layout = c.layout;
             return s->repack_stream();
@@ -1732,37 +1731,56 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
             if ((rc = try_cand(c))) break;
         }
     }
-    // Phase 3: per-colour threads per vertex, greedily colour by colour (half, same, double), in two
-    // passes over the colours; a colour's change moves the step by 1-3%, so these candidates are
-    // timed over twice the steps.  The incumbent is re-timed at that length first.
+    // Phase 3: per-colour threads per vertex.  A colour's lane count moves the step by 1-3%, about
+    // as much as the drift between timings taken a few seconds apart, so each candidate is timed
+    // alternately with the incumbent, twice each over 2 x repeats steps, and replaces it when the
+    // sums differ by more than 1%.  Greedy over the colours (lane counts 2, 4, 8, 16), two passes,
+    // restarted from uniform lanes under each factored prefetch depth (which interacts with the
+    // lane count: the 64^3 cube is fastest with the three-deep prefetch and lanes 4,8,4,8,4,4,8,8).
+    auto beats = [&](const Cand& c, const Cand& inc, bool* better) -> int {
+        float a = 0.f, b = 0.f, t = 0.f;
+        for (int r = 0; r < 2; ++r) {
+            VBD_TRY(time_of(inc, &t));
+            a += t;
+            VBD_TRY(time_of(c, &t));
+            b += t;
+        }
+        *better = b < 0.99f * a;
+        return VBD_OK;
+    };
     if (!rc && s->semantics == 0 && s->C > 1) {
         reps = 2 * repeats;
-        float ms = 0.f;
-        if (!(rc = time_of(best, &ms))) best_ms = ms;
-        for (int pass = 0; pass < 2 && !rc; ++pass) {
-            for (int col = 0; col < s->C && !rc; ++col) {
-                for (int f : {-1, 1}) {
-                    Cand c = best;
-                    if (c.colour_lanes.empty()) c.colour_lanes.assign(s->C, c.lanes);
-                    const int L = f < 0 ? c.colour_lanes[col] / 2 : c.colour_lanes[col] * 2;
-                    if (L < 2 || L > 32) continue;
-                    c.colour_lanes[col] = L;
-                    if ((rc = try_cand(c))) break;
-                }
+        std::vector<int> depths{best.prefetch};
+        if (best.layout >= 3)
+            for (int pf : {1, 2, 3})
+                if (pf != best.prefetch) depths.push_back(pf);
+        Cand overall = best;
+        float overall_ms = 1e30f;
+        for (size_t d = 0; d < depths.size() && !rc; ++d) {
+            Cand inc = best;
+            inc.prefetch = depths[d];
+            inc.colour_lanes.assign(s->C, inc.lanes);
+            for (int pass = 0; pass < 2 && !rc; ++pass)
+                for (int col = 0; col < s->C && !rc; ++col)
+                    for (int L : {2, 4, 8, 16}) {
+                        if (L == inc.colour_lanes[col]) continue;
+                        Cand c = inc;
+                        c.colour_lanes[col] = L;
+                        bool better = false;
+                        if ((rc = beats(c, inc, &better))) break;
+                        if (better) inc = c;
+                    }
+            float ms = 0.f;
+            if (!rc && !(rc = time_of(inc, &ms)) && ms < overall_ms) {
+                overall_ms = ms;
+                overall = inc;
             }
         }
-    }
-    // Phase 3b: the record prefetch again, now with the per-colour lanes (on the 64^3 cube the
-    // three-deep prefetch measured 3.80 ms/step with them against 3.85 for the two-deep one that
-    // won with uniform lanes).
-    if (!rc && best.layout >= 3) {
-        const Cand base = best;
-        for (int pf : {1, 2, 3}) {
-            if (pf == base.prefetch) continue;
-            Cand c = base;
-            c.prefetch = pf;
-            if ((rc = try_cand(c))) break;
+        if (!rc) {
+            bool better = false;
+            if (!(rc = beats(overall, best, &better)) && better) best = overall;
         }
+        if (!rc) rc = time_of(best, &best_ms);  // the incumbent at this phase's length, for phase 4
     }
     // Phase 4: the whole step as one persistent colour-walking launch (uniform lanes, no per-colour
     // shape) against the captured graph.
