@@ -511,18 +511,67 @@ def bench_batched(args, rank, world, local, stream, dist, barrier):
     }
 
 
-def bench_adjoint(local, stream):
-    """The differentiated configuration: 32x8x8 beam, per-tet materials, 30 steps x 30 iterations,
-    checkpoint every 10 steps; forward (recorded) vs backward (recompute + implicit adjoint, 50
-    Chebyshev-accelerated Gauss-Seidel sweeps per step), wall time around the C-ABI calls."""
+def bench_beam(local, stream, autotune=True):
+    """The plain beam (16x4x4 cells, 425 vertices): 100 steps x 20 iterations from rest, the
+    reference's CPU-runnable configuration, through the C ABI; wall time around the steps (the
+    positions stay on the device).  The launch configuration is the autotuner's (set-up)."""
     import torch
 
-    from vbd_tetmesh_b200 import build_solver, meshgen
+    from vbd_tetmesh_b200 import _capi, build_solver, meshgen
+
+    m = meshgen.beam()
+    st = meshgen.BEAM_SETTINGS
+    with torch.cuda.stream(stream):
+        s = build_solver(m, device=local, stream=stream.cuda_stream)
+        tuned = s.autotune(st["dt"], iterations=st["iterations"], repeats=5) if autotune else None
+        best = None
+        for _ in range(3):
+            s.set_positions(m.x)
+            s.set_velocities(m.v)
+            s.sync()
+            t0 = time.perf_counter()
+            for _ in range(st["steps"]):
+                s.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])
+            s.sync()
+            t = time.perf_counter() - t0
+            best = t if best is None else min(best, t)
+        launches_before = s.kernel_launches()
+        s.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])
+        s.sync()
+        launches = s.kernel_launches() - launches_before
+        path = {0: "captured CUDA graph", 1: "persistent kernel with grid barriers",
+                2: "cluster walk (one thread-block cluster, positions in distributed shared memory)"}[
+            s.get_option(_capi.OPT_PERSISTENT)]
+        s.close()
+    vi = m.num_verts * st["iterations"] * st["steps"]
+    return {
+        "workload": "beam 16x4x4 cells x 6 tets (425 vertices, 1,536 tets), E 1e5, nu 0.3, 100 steps x 20 "
+                    "iterations, dt 1/60, Chebyshev 0.95, from rest",
+        "ms_per_step": best * 1e3 / st["steps"],
+        "value": vi / best,
+        "unit": "vertex-iterations/s",
+        "kernel_launches_per_step": launches,
+        "path": path,
+        "autotuned": tuned,
+        "how": "wall time around 100 vbd_solver_step calls (best of 3), positions resident on the device",
+    }
+
+
+def bench_adjoint(local, stream, autotune=True):
+    """The differentiated configuration: 32x8x8 beam, per-tet materials, 30 steps x 30 iterations,
+    checkpoint every 10 steps; forward (recorded) vs backward (recompute + implicit adjoint, 50
+    Chebyshev-accelerated Gauss-Seidel sweeps per step), wall time around the C-ABI calls.  The
+    launch configuration is the autotuner's (set-up)."""
+    import torch
+
+    from vbd_tetmesh_b200 import _capi, build_solver, meshgen
 
     m, tip, target = meshgen.diff_beam()
     st = meshgen.DIFF_SETTINGS
     with torch.cuda.stream(stream):
         s = build_solver(m, device=local, stream=stream.cuda_stream)
+        tuned = s.autotune(st["dt"], iterations=st["iterations"], repeats=3) if autotune else None
+        persistent = s.get_option(_capi.OPT_PERSISTENT)
         res = []
         for _ in range(3):
             s.set_positions(m.x)
@@ -563,6 +612,8 @@ def bench_adjoint(local, stream):
         "backward_over_forward": tb / tf,
         "adjoint_sweeps_per_step": st["adjoint_iterations"],
         "adjoint_rho": st["adjoint_rho"],
+        "autotuned": tuned,
+        "forward_path": {0: "captured CUDA graph", 1: "persistent kernel", 2: "cluster walk"}[persistent],
         "accuracy": "checked in tests/test_gpu_adjoint.py: <= 1e-3 relative vs the FP64 implicit adjoint",
         "roofline": {
             "bound": "latency: 2,673 vertices give under 1% of the GPU's resident threads work",
@@ -834,7 +885,8 @@ def main():
     if not args.no_batched:
         result["batched"] = bench_batched(args, rank, world, local, stream, dist, barrier)
     if not args.no_adjoint and rank == 0:
-        result["adjoint"] = bench_adjoint(local, stream)
+        result["beam"] = bench_beam(local, stream, not args.no_autotune)
+        result["adjoint"] = bench_adjoint(local, stream, not args.no_autotune)
     if not args.no_material_id and rank == 0:
         result["material_id"] = bench_material_id(local, stream)
 

@@ -288,7 +288,19 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *   VBD_OPT_BLOCK:       threads per block of the sweep kernel: 64, 128 or 256
  *   VBD_OPT_PERSISTENT:  1 = run each step / solve as one cooperative launch that walks the colours
  *                        with a grid barrier after each one (bounded wait: a barrier that gives up
- *                        makes the next vbd_solver_sync return VBD_ERR_TIMEOUT)
+ *                        makes the next vbd_solver_sync return VBD_ERR_TIMEOUT);
+ *                        2 = run each sub-step / solve as ONE thread-block cluster that keeps both
+ *                        position buffers of the mesh (and the pre-sweep positions) in every CTA's
+ *                        shared memory, exchanges updated positions through distributed shared
+ *                        memory and separates the colours with the cluster's hardware barrier.  For
+ *                        meshes whose positions fit (48 B per vertex within the device's per-CTA
+ *                        shared memory: about 4,800 vertices on B200) with the factored records (VBD_OPT_LAYOUT 3 or
+ *                        4); VBD_ERR_INVALID_ARG otherwise.  Same results as the captured graph at the
+ *                        same lane count.  Both persistent forms use VBD_OPT_LANES for every colour
+ *                        (at least 4) and evaluate no energy history
+ *   VBD_OPT_CLUSTER_CTAS: CTAs of the cluster walk, 1-16; 0 (default) = enough 256-thread
+ *                        CTAs to sweep the largest colour in one round, at most 16.  Reading it
+ *                        back after a cluster step gives the count in use
  *   VBD_OPT_ADJOINT_ALTERNATE: 1 = adjoint sweeps alternate the colour order (a forward and a
  *                        backward sweep form one symmetric Gauss-Seidel pair)
  *   VBD_OPT_SEMANTICS:   0 = the CPU solver's (VBDsolver, VBD.cpp:114-256): Neo-Hookean element,
@@ -332,7 +344,8 @@ typedef enum vbd_option {
     VBD_OPT_L2_PREFETCH = 10,
     VBD_OPT_RECORD_CACHE = 11,
     VBD_OPT_RECORD_PERSIST_MB = 12,
-    VBD_OPT_ENERGY_EVERY = 13
+    VBD_OPT_ENERGY_EVERY = 13,
+    VBD_OPT_CLUSTER_CTAS = 14
 } vbd_option;
 int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value);
 int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value);
@@ -357,7 +370,9 @@ int vbd_solver_get_colour_lanes(vbd_solver* s, int32_t num_colours, int32_t* lan
  *      counts 2, 4, 8 and 16, two passes, restarted under each prefetch depth of the factored
  *      layouts; each candidate is timed alternately with the incumbent (twice each, 2 x repeats
  *      steps) against drift;
- *   4. the persistent colour-walking kernel (VBD_OPT_PERSISTENT) against the captured graph.
+ *   4. the persistent colour-walking kernel (VBD_OPT_PERSISTENT 1) against the captured graph,
+ *      then, where the mesh fits, the cluster walk (VBD_OPT_PERSISTENT 2) at 4, 8, 16 and 32
+ *      threads per vertex with record layouts 3 and 4.
  * Phases 2-4 replace the choice only when faster by more than 1%.  chosen (may be null) receives 5
  * ints: lanes, layout, prefetch, pdl, block; the rest of the choice is read back with
  * vbd_solver_get_option (VBD_OPT_RECORD_CACHE, VBD_OPT_PERSISTENT) and vbd_solver_get_colour_lanes. */

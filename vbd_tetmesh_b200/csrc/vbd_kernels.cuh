@@ -592,18 +592,16 @@ __device__ __forceinline__ void vertex_update(const SweepParams& p, int v, int l
 
 // The group's reduction and the first lane's block solve, Chebyshev blend and stores (the second
 // half of vertex_update).
-template <int LANES>
-__device__ __forceinline__ void vertex_solve(const SweepParams& p, int v, int lane, bool active, float4 xi, Acc& acc) {
-    group_reduce<LANES>(acc);
-    if (!active || lane != 0) return;
-
-    const float4 yi = p.y[v];
-    const float cm = yi.w * p.dtsr;
+// The block solve of one vertex from its reduced sums (VBD.cpp:141-152, Types.h:85-112): returns
+// the new position, or xi where |det H| <= 1e-8 (counted in status); flags a non-finite result.
+__device__ __forceinline__ float4 block_solve(const Acc& acc, float4 xi, float4 yi, float dtsr,
+                                              unsigned long long* status) {
+    const float cm = yi.w * dtsr;
     const float H00 = cm + acc.h00, H01 = acc.h01, H02 = acc.h02;
     const float H11 = cm + acc.h11, H12 = acc.h12, H22 = cm + acc.h22;
-    const float f0 = (yi.w * (yi.x - xi.x)) * p.dtsr - acc.g0;
-    const float f1 = (yi.w * (yi.y - xi.y)) * p.dtsr - acc.g1;
-    const float f2 = (yi.w * (yi.z - xi.z)) * p.dtsr - acc.g2;
+    const float f0 = (yi.w * (yi.x - xi.x)) * dtsr - acc.g0;
+    const float f1 = (yi.w * (yi.y - xi.y)) * dtsr - acc.g1;
+    const float f2 = (yi.w * (yi.z - xi.z)) * dtsr - acc.g2;
     // adjugate of the symmetric H
     const float A00 = H11 * H22 - H12 * H12;
     const float A01 = H02 * H12 - H01 * H22;
@@ -619,19 +617,29 @@ __device__ __forceinline__ void vertex_solve(const SweepParams& p, int v, int la
         xn.y = xi.y + inv * (A01 * f0 + A11 * f1 + A12 * f2);
         xn.z = xi.z + inv * (A02 * f0 + A12 * f1 + A22 * f2);
     } else {
-        atomicAdd(p.status + ST_SINGULAR, 1ull);
+        atomicAdd(status + ST_SINGULAR, 1ull);
     }
-    if (!(isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z))) p.status[ST_NONFINITE] = 1ull;
+    if (!(isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z))) status[ST_NONFINITE] = 1ull;
+    return xn;
+}
+
+// The Chebyshev blend x^(k) = omega (x~ - pp) + pp (VBD.cpp:290-300).
+__device__ __forceinline__ float4 cheb_blend(float4 xn, float4 q, float omega) {
+    float4 xa;
+    xa.x = omega * (xn.x - q.x) + q.x;
+    xa.y = omega * (xn.y - q.y) + q.y;
+    xa.z = omega * (xn.z - q.z) + q.z;
+    xa.w = xn.w;
+    return xa;
+}
+
+template <int LANES>
+__device__ __forceinline__ void vertex_solve(const SweepParams& p, int v, int lane, bool active, float4 xi, Acc& acc) {
+    group_reduce<LANES>(acc);
+    if (!active || lane != 0) return;
+    const float4 xn = block_solve(acc, xi, p.y[v], p.dtsr, p.status);
     p.x[v] = xn;
-    if (p.accel) {
-        const float4 q = p.pp[v];
-        float4 xa;
-        xa.x = p.omega * (xn.x - q.x) + q.x;
-        xa.y = p.omega * (xn.y - q.y) + q.y;
-        xa.z = p.omega * (xn.z - q.z) + q.z;
-        xa.w = xn.w;
-        p.xnext[v] = xa;
-    }
+    if (p.accel) p.xnext[v] = cheb_blend(xn, p.pp[v], p.omega);
     if (p.keep_pp) p.pp[v] = xi;
 }
 
@@ -1108,10 +1116,9 @@ __global__ void __launch_bounds__(256, 4) k_persistent(PersistParams p) {
 // computeInertia / savePreviousPosition, TetMesh.h:319-348).  Free vertices are [0, nfree).
 // y = x + h v is rounded after the product and after the sum (no fused multiply-add), as the
 // reference's host code computes it.
-__global__ void k_predict(const float4* __restrict__ x, float4* __restrict__ v, float4* __restrict__ xprev,
-                          float4* __restrict__ y, int nfree, int n, float h, float hgx, float hgy, float hgz) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__device__ __forceinline__ void predict_vertex(int i, const float4* __restrict__ x, float4* __restrict__ v,
+                                               float4* __restrict__ xprev, float4* __restrict__ y, int nfree, float h,
+                                               float hgx, float hgy, float hgz) {
     const float4 xi = x[i];
     xprev[i] = xi;
     float4 yi = y[i];
@@ -1132,22 +1139,28 @@ __global__ void k_predict(const float4* __restrict__ x, float4* __restrict__ v, 
     y[i] = yi;
 }
 
+__global__ void k_predict(const float4* __restrict__ x, float4* __restrict__ v, float4* __restrict__ xprev,
+                          float4* __restrict__ y, int nfree, int n, float h, float hgx, float hgy, float hgz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) predict_vertex(i, x, v, xprev, y, nfree, h, hgx, hgy, hgz);
+}
+
 // Velocity update v = (x - x_prev)/h * 0.999 (TetMesh::updateVelocity, TetMesh.h:305-311) and,
 // when the final positions sit in the second buffer, their copy back into the first.
+__device__ __forceinline__ float4 damped_velocity(float4 xi, float4 xp, float4 vi, float h) {
+    vi.x = ((xi.x - xp.x) / h) * 0.999f;
+    vi.y = ((xi.y - xp.y) / h) * 0.999f;
+    vi.z = ((xi.z - xp.z) / h) * 0.999f;
+    return vi;
+}
+
 __global__ void k_finish(const float4* __restrict__ xf, float4* __restrict__ x0, const float4* __restrict__ xprev,
                          float4* __restrict__ v, int nfree, float h, int copy_back, int update_v) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nfree) return;
     const float4 xi = xf[i];
     if (copy_back) x0[i] = xi;
-    if (update_v) {
-        const float4 xp = xprev[i];
-        float4 vi = v[i];
-        vi.x = ((xi.x - xp.x) / h) * 0.999f;
-        vi.y = ((xi.y - xp.y) / h) * 0.999f;
-        vi.z = ((xi.z - xp.z) / h) * 0.999f;
-        v[i] = vi;
-    }
+    if (update_v) v[i] = damped_velocity(xi, xprev[i], v[i], h);
 }
 
 // dst.xyz = src.xyz over [0, n), keeping dst.w (x = y start, VBD_GPU_Wrapper.cu:334).
@@ -1542,6 +1555,30 @@ __device__ __forceinline__ void fact_adjoint(const FactRec& r, float4 xi, const 
     acc.h22 += r.am + r.b * Cq[2] * Cq[2];
 }
 
+// The adjoint block solve of one vertex of mass m: (m/h^2 I + H_vv) lam = g - (the off-diagonal
+// products summed in acc.g), with the diagonal block in acc.h; lam = 0 where |det| <= 1e-30.
+__device__ __forceinline__ float4 adj_block_solve(const Acc& acc, float m, float dtsr, float4 g) {
+    const float cm = m * dtsr;
+    const float H00 = cm + acc.h00, H01 = acc.h01, H02 = acc.h02, H11 = cm + acc.h11, H12 = acc.h12, H22 = cm + acc.h22;
+    const float f0 = g.x - acc.g0, f1 = g.y - acc.g1, f2 = g.z - acc.g2;
+    const float A00 = H11 * H22 - H12 * H12, A01 = H02 * H12 - H01 * H22, A02 = H01 * H12 - H02 * H11;
+    const float A11 = H00 * H22 - H02 * H02, A12 = H02 * H01 - H00 * H12, A22 = H00 * H11 - H01 * H01;
+    const float det = H00 * A00 + H01 * A01 + H02 * A02;
+    float4 l = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (fabsf(det) > 1e-30f) {
+        const float inv = 1.0f / det;
+        l.x = inv * (A00 * f0 + A01 * f1 + A02 * f2);
+        l.y = inv * (A01 * f0 + A11 * f1 + A12 * f2);
+        l.z = inv * (A02 * f0 + A12 * f1 + A22 * f2);
+    }
+    return l;
+}
+
+// The adjoint's Chebyshev blend omega (lam~ - lam_pp) + lam_pp.
+__device__ __forceinline__ float4 adj_blend(float4 l, float4 q, float omega) {
+    return make_float4(omega * (l.x - q.x) + q.x, omega * (l.y - q.y) + q.y, omega * (l.z - q.z) + q.z, 0.f);
+}
+
 // One colour of one adjoint Gauss-Seidel sweep.  LAYOUT 0 reads tet records through inc_tet,
 // LAYOUT 2 the forward's compact incidence records; the lane's first record is fetched before the
 // programmatic-launch dependency wait, the next one while the current is evaluated.
@@ -1593,27 +1630,10 @@ __global__ void __launch_bounds__(256) k_adj_sweep(AdjParams p) {
     }
     group_reduce<LANES>(acc);
     if (!active || lane != 0) return;
-    const float cm = p.y[v].w * p.dtsr;
-    const float4 g = p.G[v];
-    const float H00 = cm + acc.h00, H01 = acc.h01, H02 = acc.h02, H11 = cm + acc.h11, H12 = acc.h12, H22 = cm + acc.h22;
-    const float f0 = g.x - acc.g0, f1 = g.y - acc.g1, f2 = g.z - acc.g2;
-    const float A00 = H11 * H22 - H12 * H12, A01 = H02 * H12 - H01 * H22, A02 = H01 * H12 - H02 * H11;
-    const float A11 = H00 * H22 - H02 * H02, A12 = H02 * H01 - H00 * H12, A22 = H00 * H11 - H01 * H01;
-    const float det = H00 * A00 + H01 * A01 + H02 * A02;
-    float4 l = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (fabsf(det) > 1e-30f) {
-        const float inv = 1.0f / det;
-        l.x = inv * (A00 * f0 + A01 * f1 + A02 * f2);
-        l.y = inv * (A01 * f0 + A11 * f1 + A12 * f2);
-        l.z = inv * (A02 * f0 + A12 * f1 + A22 * f2);
-    }
+    const float4 l = adj_block_solve(acc, p.y[v].w, p.dtsr, p.G[v]);
     const float4 lold = p.lam[v];
     p.lam[v] = l;
-    if (p.accel) {
-        const float4 q = p.lam_pp[v];
-        p.lam_next[v] = make_float4(p.omega * (l.x - q.x) + q.x, p.omega * (l.y - q.y) + q.y,
-                                    p.omega * (l.z - q.z) + q.z, 0.f);
-    }
+    if (p.accel) p.lam_next[v] = adj_blend(l, p.lam_pp[v], p.omega);
     if (p.keep_pp) p.lam_pp[v] = lold;
 }
 

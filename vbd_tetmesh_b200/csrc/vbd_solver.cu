@@ -10,6 +10,7 @@
 
 #include "vbd_b200.h"
 #include "vbd_internal.h"
+#include "vbd_cluster.cuh"
 #include "vbd_kernels.cuh"
 
 namespace vbd {
@@ -105,6 +106,15 @@ static SweepFn pick_sweep(int lanes, int layout, int prefetch, bool cache) {
     }
 }
 
+// The cluster walk reads the factored records (layouts 3 and 4).
+template <int L> static void (*pick_cluster(int layout))(PersistParams) {
+    return layout == 3 ? &k_cluster_walk<L, 3> : &k_cluster_walk<L, 4>;
+}
+
+template <int L> static void (*pick_cluster_adjoint(int layout))(AdjWalkParams) {
+    return layout == 3 ? &k_cluster_adjoint<L, 3> : &k_cluster_adjoint<L, 4>;
+}
+
 template <int L> static void (*pick_persistent(int layout))(PersistParams) {
     switch (layout) {
         case 0: return &k_persistent<L, 0>;
@@ -129,7 +139,7 @@ template <int L> static void (*pick_adj_sweep(int layout))(AdjParams) {
 struct GraphKey {
     int kind;  // 0 = step, 1 = solve, 2 = single sweep
     int iters, accel, init, lanes, layout, prefetch, pdl, block, semantics, l2_prefetch, src;
-    int record_cache, persist_mb, energy_every, pad_;
+    int record_cache, persist_mb, energy_every, walk;  // walk: 2 = the adjoint sweeps as a cluster walk
     unsigned long long colour_shape;  // hash of the per-colour lanes (0 = uniform) and the mesh
     float h, dtsr, hg[3], rho;
     bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
@@ -206,7 +216,14 @@ struct vbd_solver {
     float omega_next(int k, float rho, float prev) const {
         return semantics ? vbd::omega_of_wrapper(k, rho, prev) : vbd::omega_of(k, rho, prev);
     }
-    int persistent = 0;                             // whole step in one cooperative launch
+    // whole step in one launch: 1 = cooperative kernel with grid barriers, 2 = one thread-block
+    // cluster holding the positions in shared memory (meshes of up to about 7,000 vertices)
+    int persistent = 0;
+    int cluster_ctas_opt = 0;                       // CTAs of the cluster walk (0 = from the colour sizes)
+    int cl_ctas = 0, cl_block = 0, cl_lanes = 0, cl_gen = -1, cl_req = 0;  // launch shape resolved for the mesh
+    int ca_ctas = 0, ca_lanes = 0, ca_gen = -1, ca_req = 0;                // the same for the adjoint walk
+    vbd::DBuf<float> d_adj_omega;
+    std::vector<float> adj_omega_cache;
     long long spin_limit = 1LL << 22;               // barrier polls before a persistent launch gives up
     vbd::DBuf<int> d_cstart;
     vbd::DBuf<float> d_omega;
@@ -483,9 +500,8 @@ struct vbd_solver {
         return w;
     }
 
-    int launch_persistent(int iters, float dtsr, bool accel, float rho, bool predict, bool finish, bool from_inertia,
-                          float h, const float* hg, int expected_extra = 0) {
-        if (!barrier.p) VBD_TRY(barrier.alloc(1));
+    // The colour starts and the Chebyshev schedule on the device, for the single-launch walks.
+    int upload_schedule(int iters, bool accel, float rho) {
         if (d_cstart.n != cstart.size()) {
             VBD_TRY(d_cstart.alloc(cstart.size()));
             CUDA_TRY(cudaMemcpy(d_cstart.p, cstart.data(), sizeof(int) * cstart.size(), cudaMemcpyHostToDevice));
@@ -497,6 +513,39 @@ struct vbd_solver {
             CUDA_TRY(cudaStreamSynchronize(stream));
             omega_cache = w;
         }
+        return VBD_OK;
+    }
+
+    // The parameters of a single-launch walk (the persistent kernel or the cluster walk).
+    vbd::PersistParams walk_params(int iters, float dtsr, bool accel, bool predict, bool finish, bool from_inertia,
+                                   float h, const float* hg) const {
+        vbd::PersistParams w{};
+        w.sw = vbd::SweepParams{x0.p, x1.p, pp.p, y.p,  inc_off.p, inc_tet.p, rec.p, irec.p, crec.p, cmat.p,
+                                status.p, 0,  0,    dtsr, 1.0f,      0,         accel ? 1 : 0, 0, 0};
+        w.xa = x0.p;
+        w.xb = x1.p;
+        w.v = v.p;
+        w.xprev = xprev.p;
+        w.cstart = d_cstart.p;
+        w.omega = d_omega.p;
+        w.ncol = C;
+        w.iters = iters;
+        w.nfree = nfree;
+        w.n = N;
+        w.predict = predict ? 1 : 0;
+        w.finish = finish ? 1 : 0;
+        w.init_from_inertia = from_inertia ? 1 : 0;
+        w.h = h;
+        w.hgx = hg ? hg[0] : 0.f;
+        w.hgy = hg ? hg[1] : 0.f;
+        w.hgz = hg ? hg[2] : 0.f;
+        return w;
+    }
+
+    int launch_persistent(int iters, float dtsr, bool accel, float rho, bool predict, bool finish, bool from_inertia,
+                          float h, const float* hg, int expected_extra = 0) {
+        if (!barrier.p) VBD_TRY(barrier.alloc(1));
+        VBD_TRY(upload_schedule(iters, accel, rho));
         const int L = lanes < 4 ? 4 : lanes;
         const int threads = 256;
         void (*fn)(vbd::PersistParams) = nullptr;
@@ -511,33 +560,204 @@ struct vbd_solver {
         CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
         if (per_sm < 1) VBD_FAIL(VBD_ERR_CUDA, "persistent kernel cannot be resident");
         const int grid = per_sm * sms;
-        vbd::PersistParams pp_{};
-        pp_.sw = vbd::SweepParams{x0.p, x1.p, pp.p, y.p,  inc_off.p, inc_tet.p, rec.p, irec.p, crec.p, cmat.p,
-                                  status.p, 0,  0,    dtsr, 1.0f,      0,         accel ? 1 : 0, 0, 0};
-        pp_.xa = x0.p;
-        pp_.xb = x1.p;
-        pp_.v = v.p;
-        pp_.xprev = xprev.p;
-        pp_.cstart = d_cstart.p;
-        pp_.omega = d_omega.p;
+        vbd::PersistParams pp_ = walk_params(iters, dtsr, accel, predict, finish, from_inertia, h, hg);
         pp_.bar = barrier.p;
         pp_.spin_limit = spin_limit;
-        pp_.ncol = C;
-        pp_.iters = iters;
-        pp_.nfree = nfree;
-        pp_.n = N;
-        pp_.predict = predict ? 1 : 0;
-        pp_.finish = finish ? 1 : 0;
-        pp_.init_from_inertia = from_inertia ? 1 : 0;
         pp_.expected_blocks = grid + expected_extra;
-        pp_.h = h;
-        pp_.hgx = hg ? hg[0] : 0.f;
-        pp_.hgy = hg ? hg[1] : 0.f;
-        pp_.hgz = hg ? hg[2] : 0.f;
         CUDA_TRY(cudaMemsetAsync(barrier.p, 0, sizeof(vbd::GridBarrier), stream));
         void* args[] = {&pp_};
         CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(fn), dim3(grid), dim3(threads), args, 0, stream));
         return check_launch();
+    }
+
+    // The cluster walk holds both position buffers of the mesh and the pre-sweep positions in each
+    // CTA's shared memory.
+    size_t cluster_smem() const { return 3 * sizeof(float4) * (size_t)N; }
+    bool cluster_fit(const char** why) const {
+        if (semantics) {
+            *why = "the cluster walk runs the VBDsolver semantics only";
+            return false;
+        }
+        if (layout != 3 && layout != 4) {
+            *why = "the cluster walk reads the factored records (VBD_OPT_LAYOUT 3 or 4)";
+            return false;
+        }
+        int optin = 0;
+        if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess ||
+            cluster_smem() + 64 > (size_t)optin) {  // + the walk's two mbarriers
+            *why = "the mesh's positions (48 B per vertex) do not fit in one CTA's shared memory";
+            return false;
+        }
+        return true;
+    }
+
+    // CTAs of the cluster walk: enough 256-thread CTAs for the largest colour in one round, at most
+    // 16, fewer when the device cannot hold a cluster of that size.
+    template <class Params>
+    int cluster_ctas_for(void (*fn)(Params), int L, size_t smem, int* out) {
+        int maxcol = 1;
+        for (int c = 0; c < C; ++c) maxcol = std::max(maxcol, cstart[c + 1] - cstart[c]);
+        const long long need = (long long)maxcol * L;
+        const int block = vbd::kClusterMaxBlock;
+        int ctas = cluster_ctas_opt > 0 ? cluster_ctas_opt : (int)std::min<long long>(16, (need + block - 1) / block);
+        ctas = std::max(ctas, 1);
+        CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeNonPortableClusterSizeAllowed,
+                                      1));
+        for (; ctas >= 1; --ctas) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(ctas);
+            cfg.blockDim = dim3(block);
+            cfg.dynamicSmemBytes = smem;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = ctas;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int clusters = 0;
+            const cudaError_t e = cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg);
+            if (e == cudaSuccess && clusters >= 1) break;
+            (void)cudaGetLastError();
+            if (cluster_ctas_opt > 0) VBD_FAIL(VBD_ERR_INVALID_ARG, "a cluster of %d CTAs cannot be resident", ctas);
+        }
+        if (ctas < 1) VBD_FAIL(VBD_ERR_CUDA, "the cluster walk cannot be resident");
+        *out = ctas;
+        return VBD_OK;
+    }
+
+    int resolve_cluster(void (*fn)(vbd::PersistParams), int L) {
+        if (cl_gen == shape_gen && cl_lanes == L && cl_req == cluster_ctas_opt && cl_ctas > 0) return VBD_OK;
+        VBD_TRY(cluster_ctas_for(fn, L, cluster_smem(), &cl_ctas));
+        cl_block = vbd::kClusterMaxBlock;
+        cl_lanes = L;
+        cl_gen = shape_gen;
+        cl_req = cluster_ctas_opt;
+        return VBD_OK;
+    }
+
+    // The adjoint walk holds X, both adjoint buffers and the pre-sweep adjoint: 64 B per vertex.
+    size_t cluster_adj_smem() const { return 4 * sizeof(float4) * (size_t)N; }
+    bool cluster_adj_fit() const {
+        int optin = 0;
+        return semantics == 0 && (layout == 3 || layout == 4) &&
+               cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) == cudaSuccess &&
+               cluster_adj_smem() + 64 <= (size_t)optin;
+    }
+    // With the cluster walk selected, the adjoint sweeps of a sub-step run as one cluster launch
+    // too where the mesh fits.
+    bool adj_walk() const { return persistent == 2 && !timing && cluster_adj_fit(); }
+
+    // Set-up of the adjoint walk outside any graph capture: the sweep schedule on the device and
+    // the cluster shape.
+    int prepare_adj_walk(int sweeps, float rho, void (**fn_out)(vbd::AdjWalkParams)) {
+        std::vector<float> w(std::max(sweeps, 1), 1.0f);
+        float omega = 1.0f;
+        for (int it = 1; it <= sweeps; ++it) {
+            if (rho > 0.0f) omega = vbd::omega_of(it, rho, omega);
+            w[it - 1] = rho > 0.0f ? omega : 1.0f;
+        }
+        if (w != adj_omega_cache) {
+            if (d_adj_omega.n < w.size()) VBD_TRY(d_adj_omega.alloc(w.size()));
+            CUDA_TRY(cudaMemcpyAsync(d_adj_omega.p, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice, stream));
+            CUDA_TRY(cudaStreamSynchronize(stream));
+            adj_omega_cache = w;
+        }
+        if (d_cstart.n != cstart.size()) {
+            VBD_TRY(d_cstart.alloc(cstart.size()));
+            CUDA_TRY(cudaMemcpy(d_cstart.p, cstart.data(), sizeof(int) * cstart.size(), cudaMemcpyHostToDevice));
+        }
+        const int L = lanes < 4 ? 4 : lanes;
+        void (*fn)(vbd::AdjWalkParams) = nullptr;
+        switch (L) {
+            case 4: fn = vbd::pick_cluster_adjoint<4>(layout); break;
+            case 8: fn = vbd::pick_cluster_adjoint<8>(layout); break;
+            case 16: fn = vbd::pick_cluster_adjoint<16>(layout); break;
+            default: fn = vbd::pick_cluster_adjoint<32>(layout); break;
+        }
+        if (!(ca_gen == shape_gen && ca_lanes == L && ca_req == cluster_ctas_opt && ca_ctas > 0)) {
+            VBD_TRY(cluster_ctas_for(fn, L, cluster_adj_smem(), &ca_ctas));
+            ca_lanes = L;
+            ca_gen = shape_gen;
+            ca_req = cluster_ctas_opt;
+        }
+        *fn_out = fn;
+        return VBD_OK;
+    }
+
+    // The adjoint sweeps of one sub-step as one cluster launch, from the live buffer adj_cur.
+    int launch_cluster_adjoint(void (*fn)(vbd::AdjWalkParams), const TapeStep& t, const float4* X, int sweeps,
+                               float rho) {
+        vbd::AdjWalkParams w{};
+        w.a = vbd::AdjParams{X,      nullptr, adj_G.p, y.p,  inc_off.p, inc_tet.p, rec.p,
+                             crec.p, cmat.p,  t.dtsr,  0,    0,         nullptr,   nullptr,
+                             1.0f,   0,       0};
+        w.lam0 = adj_cur ? adj_lam2.p : adj_lam.p;
+        w.lam1 = adj_cur ? adj_lam.p : adj_lam2.p;
+        w.cstart = d_cstart.p;
+        w.omega = d_adj_omega.p;
+        w.status = status.p;
+        w.ncol = C;
+        w.sweeps = sweeps;
+        w.n = N;
+        w.nfree = nfree;
+        w.keep_pp = rho > 0.0f ? 1 : 0;
+        w.alternate = adj_alternate;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(ca_ctas);
+        cfg.blockDim = dim3(vbd::kClusterMaxBlock);
+        cfg.dynamicSmemBytes = cluster_adj_smem();
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = ca_ctas;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CUDA_TRY(cudaLaunchKernelEx(&cfg, fn, w));
+        return check_launch();
+    }
+
+    // A sub-step (predict and finish) or a solve as one cluster launch (vbd::k_cluster_walk).
+    int launch_cluster(int iters, float dtsr, bool accel, float rho, bool predict, bool finish, bool from_inertia,
+                       float h, const float* hg) {
+        const char* why = nullptr;
+        if (!cluster_fit(&why)) VBD_FAIL(VBD_ERR_INVALID_ARG, "%s", why);
+        VBD_TRY(upload_schedule(iters, accel, rho));
+        const int L = lanes < 4 ? 4 : lanes;
+        void (*fn)(vbd::PersistParams) = nullptr;
+        switch (L) {
+            case 4: fn = vbd::pick_cluster<4>(layout); break;
+            case 8: fn = vbd::pick_cluster<8>(layout); break;
+            case 16: fn = vbd::pick_cluster<16>(layout); break;
+            default: fn = vbd::pick_cluster<32>(layout); break;
+        }
+        VBD_TRY(resolve_cluster(fn, L));
+        const vbd::PersistParams w = walk_params(iters, dtsr, accel, predict, finish, from_inertia, h, hg);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(cl_ctas);
+        cfg.blockDim = dim3(cl_block);
+        cfg.dynamicSmemBytes = cluster_smem();
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cl_ctas;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CUDA_TRY(cudaLaunchKernelEx(&cfg, fn, w));
+        return check_launch();
+    }
+
+    // A sub-step or solve through the single-launch walk VBD_OPT_PERSISTENT selects.
+    int launch_walk(int iters, float dtsr, bool accel, float rho, bool predict, bool finish, bool from_inertia,
+                    float h, const float* hg) {
+        if (persistent == 2) return launch_cluster(iters, dtsr, accel, rho, predict, finish, from_inertia, h, hg);
+        return launch_persistent(iters, dtsr, accel, rho, predict, finish, from_inertia, h, hg);
     }
 
     int snapshot(vbd::DBuf<float4>& dst) {
@@ -577,7 +797,7 @@ struct vbd_solver {
         key.hg[2] = t.hg[2];
         key.rho = t.rho;
         if (persistent && !timing)
-            return launch_persistent(t.iters, t.dtsr, t.accel != 0, t.rho, true, true, false, t.h, t.hg);
+            return launch_walk(t.iters, t.dtsr, t.accel != 0, t.rho, true, true, false, t.h, t.hg);
         return run(key, [&] { return emit_substep(t.h, t.dtsr, t.hg, t.iters, t.accel != 0, t.rho); });
     }
 
@@ -585,7 +805,8 @@ struct vbd_solver {
     // sweeps on (M/h^2 + H) lam = x~ + c v~ with the Chebyshev blend of weight schedule
     // getAcceleratorOmega(k, rho) (rho = 0: plain Gauss-Seidel), then the parameter gradients, the
     // pinned-vertex coupling and the step's adjoint update.
-    int emit_adjoint_substep(const TapeStep& t, const float4* X, int sweeps, float rho) {
+    int emit_adjoint_substep(const TapeStep& t, const float4* X, int sweeps, float rho,
+                             void (*walk)(vbd::AdjWalkParams) = nullptr) {
         const float c = 0.999f / t.h;
         const int L = lanes < 4 ? 4 : lanes;
         vbd::k_adj_rhs<<<vbd::nblk(std::max(nfree, 1), 256), 256, 0, stream>>>(adj_ax.p, adj_av.p, adj_G.p, c, nfree);
@@ -593,7 +814,15 @@ struct vbd_solver {
         int cur = adj_cur;
         float omega = 1.0f;
         const bool accel = rho > 0.0f;
-        for (int it = 1; it <= sweeps; ++it) {
+        if (walk) {
+            // all sweeps in one cluster launch; the live buffer afterwards follows the same flips
+            VBD_TRY(launch_cluster_adjoint(walk, t, X, sweeps, rho));
+            for (int it = 1; it <= sweeps && accel; ++it) {
+                omega = vbd::omega_of(it, rho, omega);
+                if (omega > 1.0f) cur ^= 1;
+            }
+        }
+        for (int it = 1; it <= sweeps && !walk; ++it) {
             bool blend = false;
             if (accel) {
                 omega = vbd::omega_of(it, rho, omega);
@@ -669,7 +898,13 @@ struct vbd_solver {
         key.h = t.h;
         key.dtsr = t.dtsr;
         key.rho = rho;
-        VBD_TRY(run(key, [&] { return emit_adjoint_substep(t, X, sweeps, rho); }));
+        void (*walk)(vbd::AdjWalkParams) = nullptr;
+        if (adj_walk()) {
+            VBD_TRY(prepare_adj_walk(sweeps, rho, &walk));
+            key.walk = 2;
+            key.block = ca_ctas;
+        }
+        VBD_TRY(run(key, [&] { return emit_adjoint_substep(t, X, sweeps, rho, walk); }));
         float omega = 1.0f;
         for (int it = 1; it <= sweeps && rho > 0.0f; ++it) {
             omega = vbd::omega_of(it, rho, omega);
@@ -1192,8 +1427,8 @@ int vbd_solver_solve(vbd_solver* s, int32_t iterations, float dt_sqr_reciprocal,
     key.dtsr = dt_sqr_reciprocal;
     key.rho = rho;
     if (s->persistent && !s->timing)
-        return s->launch_persistent(iterations, dt_sqr_reciprocal, use_acceleration != 0, rho, false, false,
-                                    init_mode == VBD_INIT_FROM_INERTIA, 1.0f, nullptr);
+        return s->launch_walk(iterations, dt_sqr_reciprocal, use_acceleration != 0, rho, false, false,
+                              init_mode == VBD_INIT_FROM_INERTIA, 1.0f, nullptr);
     return s->run(key, [&] { return s->emit_solve(iterations, dt_sqr_reciprocal, use_acceleration != 0, rho, init_mode); });
 }
 
@@ -1239,7 +1474,7 @@ int vbd_solver_step(vbd_solver* s, float dt, int32_t substeps, int32_t iteration
         // the persistent kernel evaluates no energies: with an energy history the step runs as
         // separate launches
         if (s->persistent && !s->timing && nenergy == 0)
-            VBD_TRY(s->launch_persistent(iterations, dtsr, use_acceleration != 0, rho, true, true, false, h, hg));
+            VBD_TRY(s->launch_walk(iterations, dtsr, use_acceleration != 0, rho, true, true, false, h, hg));
         else
             VBD_TRY(s->run(key, [&] {
                 return s->emit_substep(h, dtsr, hg, iterations, use_acceleration != 0, rho, nenergy > 0);
@@ -1392,7 +1627,7 @@ int vbd_solver_sync(vbd_solver* s) {
         CUDA_TRY(cudaMemcpy(&t, s->status.p + vbd::ST_TIMEOUT, sizeof(t), cudaMemcpyDeviceToHost));
         if (t) {
             CUDA_TRY(cudaMemset(s->status.p + vbd::ST_TIMEOUT, 0, sizeof(t)));
-            VBD_FAIL(VBD_ERR_TIMEOUT, "a grid barrier of the persistent kernel gave up waiting");
+            VBD_FAIL(VBD_ERR_TIMEOUT, "a wait of the persistent kernel or the cluster walk gave up");
         }
     }
     return VBD_OK;
@@ -1505,9 +1740,18 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
             s->pdl = value ? 1 : 0;
             return VBD_OK;
         case VBD_OPT_PERSISTENT:
+            if (value < 0 || value > 2) VBD_FAIL(VBD_ERR_INVALID_ARG, "persistent must be 0, 1 or 2");
             if (value && s->semantics)
                 VBD_FAIL(VBD_ERR_INVALID_ARG, "the persistent kernel runs the VBDsolver semantics only");
-            s->persistent = value ? 1 : 0;
+            if (value == 2 && s->ready) {
+                const char* why = nullptr;
+                if (!s->cluster_fit(&why)) VBD_FAIL(VBD_ERR_INVALID_ARG, "%s", why);
+            }
+            s->persistent = value;
+            return VBD_OK;
+        case VBD_OPT_CLUSTER_CTAS:
+            if (value < 0 || value > 16) VBD_FAIL(VBD_ERR_INVALID_ARG, "cluster CTAs must be 0 (automatic) to 16");
+            s->cluster_ctas_opt = value;
             return VBD_OK;
         case VBD_OPT_L2_PREFETCH:
             s->l2_prefetch = value ? 1 : 0;
@@ -1562,6 +1806,7 @@ int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value) {
         case VBD_OPT_PDL: *value = s->pdl; return VBD_OK;
         case VBD_OPT_BLOCK: *value = s->block; return VBD_OK;
         case VBD_OPT_PERSISTENT: *value = s->persistent; return VBD_OK;
+        case VBD_OPT_CLUSTER_CTAS: *value = s->persistent == 2 && s->cl_ctas > 0 ? s->cl_ctas : s->cluster_ctas_opt; return VBD_OK;
         case VBD_OPT_SEMANTICS: *value = s->semantics; return VBD_OK;
         case VBD_OPT_L2_PREFETCH: *value = s->l2_prefetch; return VBD_OK;
         case VBD_OPT_ADJOINT_ALTERNATE: *value = s->adj_alternate; return VBD_OK;
@@ -1785,10 +2030,29 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
     // Phase 4: the whole step as one persistent colour-walking launch (uniform lanes, no per-colour
     // shape) against the captured graph.
     if (!rc && s->semantics == 0) {
-        Cand c = best;
+        const Cand base = best;
+        Cand c = base;
         c.persistent = 1;
         c.colour_lanes.clear();
         rc = try_cand(c);
+        // the cluster walk, for a mesh whose positions fit in one CTA's shared memory: each lane count
+        // with either factored layout (the stored det M of layout 3 saves a division per record,
+        // which counts where the records stay in L2)
+        const char* why = nullptr;
+        if (!rc && base.layout >= 3 && s->cluster_fit(&why)) {
+            for (int lay : {3, 4}) {
+                if (lay == 4 && s->N > vbd::kPackedMaxVertices) continue;
+                for (int L : {4, 8, 16, 32}) {
+                    Cand k = base;
+                    k.persistent = 2;
+                    k.lanes = L;
+                    k.layout = lay;
+                    k.colour_lanes.clear();
+                    if ((rc = try_cand(k))) break;
+                }
+                if (rc) break;
+            }
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
