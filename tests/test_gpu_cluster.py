@@ -141,3 +141,20 @@ def test_cluster_walk_refuses_meshes_that_do_not_fit(gpu_device):
     with pytest.raises(_capi.VBDError):
         s.step(1 / 60, 5, (0.0, -9.8, 0.0), True, 0.9)
     s.close()
+
+
+def test_beam_autotune_with_cluster_candidates_completes(gpu_device):
+    """The autotuner on the beam tries the cluster walk with up to 9 CTAs for colours of 29-72
+    vertices, so CTAs finish a colour at very different times.  Every colour's bytes must be
+    announced on the receiving CTA before any CTA can send them; an earlier announcement order let
+    st.async bytes arrive first, and a bounded mbarrier wait gave up (VBD_ERR_TIMEOUT)."""
+    m = meshgen.beam()
+    st = meshgen.BEAM_SETTINGS
+    s = build_solver(m)
+    for _ in range(2):
+        chosen = s.autotune(st["dt"], iterations=st["iterations"], repeats=5)
+        assert chosen["persistent"] in (0, 1, 2)
+    s.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])
+    s.sync()
+    assert s.status() == (0, False)
+    s.close()

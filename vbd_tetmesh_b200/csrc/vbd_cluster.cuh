@@ -15,7 +15,8 @@
 //     iteration blends) and waits on its own mbarrier for them, then sweeps colour c + 1.  No
 //     cluster-wide barrier or memory fence sits between colours.  Two mbarriers alternate by
 //     colour, because a CTA that has all of colour c may send colour c + 1 before a slower CTA
-//     has finished waiting for colour c;
+//     has finished waiting for colour c, and each colour's bytes are announced on the receiving
+//     CTA before any CTA can send them (see k_cluster_walk);
 //   * while waiting, each thread loads the next colour's element records, inertial target and
 //     pre-sweep position, so their latency overlaps the wait.
 // Why the in-place sweep stays exact: a CTA sends its colour-c results only after it has read
@@ -97,7 +98,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 
 // Waits for the mbarrier phase of `parity`.  Bounded: after kClusterWaitNs, or once any thread of
-// the launch has given up (status[ST_TIMEOUT], checked every 256 polls), it sets that flag and
+// the launch has given up (status[ST_WALK_TIMEOUT], checked every 256 polls), it sets that flag and
 // returns false.  The decision is made warp-wide so the warp's shuffles stay converged.
 constexpr unsigned long long kClusterWaitNs = 1000000000ull;  // 1 s
 __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long* status) {
@@ -108,12 +109,12 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigne
             done = mbar_try(bar, parity);
             if (!done && (i & 255u) == 0u &&
                 (global_ns() - t0 > kClusterWaitNs ||
-                 *reinterpret_cast<volatile unsigned long long*>(status + ST_TIMEOUT) != 0ull))
+                 *reinterpret_cast<volatile unsigned long long*>(status + ST_WALK_TIMEOUT) != 0ull))
                 break;
         }
     }
     done = __all_sync(0xffffffffu, done);
-    if (!done) atomicOr(reinterpret_cast<unsigned int*>(status + ST_TIMEOUT), 1u);
+    if (!done) atomicOr(reinterpret_cast<unsigned int*>(status + ST_WALK_TIMEOUT), 1u);
     return done;
 }
 
@@ -195,6 +196,14 @@ __device__ __forceinline__ void cluster_vertex(const PersistParams& p, const flo
     }
 }
 
+// Bytes colour g (counted over all iterations) brings to every CTA: 16 per vertex of the colour,
+// 32 when its iteration blends.
+__device__ __forceinline__ unsigned walk_bytes(const PersistParams& p, unsigned g) {
+    const int k = (int)(g / (unsigned)p.ncol), c = (int)(g % (unsigned)p.ncol);
+    const int size = __ldg(p.cstart + c + 1) - __ldg(p.cstart + c);
+    return (unsigned)size * (__ldg(p.omega + k) > 1.0f ? 32u : 16u);
+}
+
 // A whole sub-step (or solve) of one mesh in one cluster: the predictor (or the x = y start),
 // `iters` Gauss-Seidel iterations over the colours with the Chebyshev schedule, the velocity
 // update.  Launched as one cluster of gridDim.x CTAs with 3 * n float4 of dynamic shared memory.
@@ -219,9 +228,17 @@ __global__ void __launch_bounds__(kClusterMaxBlock, 1) k_cluster_walk(PersistPar
     const int ngroups = nthreads / LANES;
     float4* y = const_cast<float4*>(p.sw.y);
     const unsigned bar0 = (unsigned)__cvta_generic_to_shared(&mbar[0]);
+    // Colour g completes on mbar[g & 1].  Its bytes are announced (expect_tx) before any CTA can
+    // send them: colours 0 and 1 here, before the cluster barrier below; colour g + 2 by this CTA
+    // once colour g is complete here and before this CTA sends anything of colour g + 1 (the
+    // __syncthreads_and after each wait orders the two), while other CTAs send colour g + 2 only
+    // after they hold all of colour g + 1.
+    const unsigned total = (unsigned)max(p.iters, 0) * (unsigned)p.ncol;
     if (tid == 0) {
         mbar_init(bar0);
         mbar_init(bar0 + 8);
+        if (total > 0) mbar_expect(bar0, walk_bytes(p, 0));
+        if (total > 1) mbar_expect(bar0 + 8, walk_bytes(p, 1));
         fence_mbar_init();
     }
 
@@ -272,7 +289,6 @@ __global__ void __launch_bounds__(kClusterMaxBlock, 1) k_cluster_walk(PersistPar
         for (int c = 0; c < p.ncol; ++c, ++gc) {
             const int vb = __ldg(p.cstart + c), ve = __ldg(p.cstart + c + 1);
             const unsigned bar = bar0 + 8u * (gc & 1u);
-            if (tid == 0) mbar_expect(bar, (unsigned)(ve - vb) * (blend ? 32u : 16u));
             const int rounds = (ve - vb + ngroups - 1) / ngroups;
             for (int r = 0; r < rounds; ++r) {
                 const int v = vb + r * ngroups + grp;
@@ -292,10 +308,10 @@ __global__ void __launch_bounds__(kClusterMaxBlock, 1) k_cluster_walk(PersistPar
                 const int v = __ldg(p.cstart + cn) + grp;
                 load_ahead<LANES, LAYOUT>(p, spp, v, v < __ldg(p.cstart + cn + 1), lane, ah);
             }
-            if (!mbar_wait(bar, (gc >> 1) & 1u, p.sw.status)) {
-                alive = false;
-                break;
-            }
+            const bool ok = mbar_wait(bar, (gc >> 1) & 1u, p.sw.status);
+            if (tid == 0 && ok && gc + 2 < total) mbar_expect(bar, walk_bytes(p, gc + 2));
+            alive = __syncthreads_and(ok) != 0;
+            if (!alive) break;
         }
         if (blend) cur ^= 1;
     }
@@ -408,6 +424,14 @@ __device__ __forceinline__ int adj_colour(const AdjWalkParams& p, int it, int k)
     return (p.alternate && (it % 2 == 0)) ? p.ncol - 1 - k : k;
 }
 
+// Bytes the g-th colour swept (over all sweeps) brings to every CTA.
+__device__ __forceinline__ unsigned adj_walk_bytes(const AdjWalkParams& p, unsigned g) {
+    const int it = (int)(g / (unsigned)p.ncol) + 1;
+    const int col = adj_colour(p, it, (int)(g % (unsigned)p.ncol));
+    const int size = __ldg(p.cstart + col + 1) - __ldg(p.cstart + col);
+    return (unsigned)size * (__ldg(p.omega + it - 1) > 1.0f ? 32u : 16u);
+}
+
 template <int LANES, int LAYOUT>
 __global__ void __launch_bounds__(kClusterMaxBlock, 1) k_cluster_adjoint(AdjWalkParams p) {
     extern __shared__ float4 sx[];  // [0, n): X, [n, 2n) and [2n, 3n): lam buffers, [3n, 4n): lam_pp
@@ -425,9 +449,13 @@ __global__ void __launch_bounds__(kClusterMaxBlock, 1) k_cluster_adjoint(AdjWalk
     const int grp = gt / LANES;
     const int ngroups = nthreads / LANES;
     const unsigned bar0 = (unsigned)__cvta_generic_to_shared(&mbar[0]);
+    // the byte announcements follow the forward walk's order (k_cluster_walk)
+    const unsigned total = (unsigned)max(p.sweeps, 0) * (unsigned)p.ncol;
     if (tid == 0) {
         mbar_init(bar0);
         mbar_init(bar0 + 8);
+        if (total > 0) mbar_expect(bar0, adj_walk_bytes(p, 0));
+        if (total > 1) mbar_expect(bar0 + 8, adj_walk_bytes(p, 1));
         fence_mbar_init();
     }
     // both buffers start from the entry adjoint (pinned entries are 0 and stay 0)
@@ -458,7 +486,6 @@ __global__ void __launch_bounds__(kClusterMaxBlock, 1) k_cluster_adjoint(AdjWalk
             const int col = adj_colour(p, it, k);
             const int vb = __ldg(p.cstart + col), ve = __ldg(p.cstart + col + 1);
             const unsigned bar = bar0 + 8u * (gc & 1u);
-            if (tid == 0) mbar_expect(bar, (unsigned)(ve - vb) * (blend ? 32u : 16u));
             const int rounds = (ve - vb + ngroups - 1) / ngroups;
             for (int r = 0; r < rounds; ++r) {
                 const int v = vb + r * ngroups + grp;
@@ -480,10 +507,10 @@ __global__ void __launch_bounds__(kClusterMaxBlock, 1) k_cluster_adjoint(AdjWalk
                 const int v = __ldg(p.cstart + cn) + grp;
                 load_adj_ahead<LANES, LAYOUT>(p, spp, v, v < __ldg(p.cstart + cn + 1), lane, ah);
             }
-            if (!mbar_wait(bar, (gc >> 1) & 1u, p.status)) {
-                alive = false;
-                break;
-            }
+            const bool ok = mbar_wait(bar, (gc >> 1) & 1u, p.status);
+            if (tid == 0 && ok && gc + 2 < total) mbar_expect(bar, adj_walk_bytes(p, gc + 2));
+            alive = __syncthreads_and(ok) != 0;
+            if (!alive) break;
         }
         if (blend) cur ^= 1;
     }

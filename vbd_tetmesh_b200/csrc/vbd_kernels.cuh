@@ -29,7 +29,9 @@ struct __align__(16) TetRec {
 };
 static_assert(sizeof(TetRec) == 64, "TetRec must be 64 bytes");
 
-enum StatusSlot { ST_SINGULAR = 0, ST_NONFINITE = 1, ST_TIMEOUT = 2, ST_SLOTS = 4 };
+// ST_TIMEOUT: a grid barrier of the persistent kernel gave up; ST_WALK_TIMEOUT: an mbarrier wait
+// of a cluster walk gave up.
+enum StatusSlot { ST_SINGULAR = 0, ST_NONFINITE = 1, ST_TIMEOUT = 2, ST_WALK_TIMEOUT = 3, ST_SLOTS = 4 };
 
 struct SweepParams {
     float4* x;                 // positions being swept in place (Gauss-Seidel)

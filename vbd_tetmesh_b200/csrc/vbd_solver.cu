@@ -220,8 +220,12 @@ struct vbd_solver {
     // cluster holding the positions in shared memory (meshes of up to about 7,000 vertices)
     int persistent = 0;
     int cluster_ctas_opt = 0;                       // CTAs of the cluster walk (0 = from the colour sizes)
-    int cl_ctas = 0, cl_block = 0, cl_lanes = 0, cl_gen = -1, cl_req = 0;  // launch shape resolved for the mesh
-    int ca_ctas = 0, ca_lanes = 0, ca_gen = -1, ca_req = 0;                // the same for the adjoint walk
+    // launch shape resolved for the mesh, the kernel and the requested CTAs (the kernel's shared-memory
+    // and cluster-size attributes are set per kernel)
+    int cl_ctas = 0, cl_block = 0, cl_gen = -1, cl_req = 0;
+    const void* cl_fn = nullptr;
+    int ca_ctas = 0, ca_gen = -1, ca_req = 0;  // the same for the adjoint walk
+    const void* ca_fn = nullptr;
     vbd::DBuf<float> d_adj_omega;
     std::vector<float> adj_omega_cache;
     long long spin_limit = 1LL << 22;               // barrier polls before a persistent launch gives up
@@ -629,10 +633,12 @@ struct vbd_solver {
     }
 
     int resolve_cluster(void (*fn)(vbd::PersistParams), int L) {
-        if (cl_gen == shape_gen && cl_lanes == L && cl_req == cluster_ctas_opt && cl_ctas > 0) return VBD_OK;
+        const void* f = reinterpret_cast<const void*>(fn);
+        if (cl_gen == shape_gen && cl_fn == f && cl_req == cluster_ctas_opt && cl_ctas > 0) return VBD_OK;
+        cl_ctas = 0;
         VBD_TRY(cluster_ctas_for(fn, L, cluster_smem(), &cl_ctas));
         cl_block = vbd::kClusterMaxBlock;
-        cl_lanes = L;
+        cl_fn = f;
         cl_gen = shape_gen;
         cl_req = cluster_ctas_opt;
         return VBD_OK;
@@ -677,9 +683,11 @@ struct vbd_solver {
             case 16: fn = vbd::pick_cluster_adjoint<16>(layout); break;
             default: fn = vbd::pick_cluster_adjoint<32>(layout); break;
         }
-        if (!(ca_gen == shape_gen && ca_lanes == L && ca_req == cluster_ctas_opt && ca_ctas > 0)) {
+        const void* f = reinterpret_cast<const void*>(fn);
+        if (!(ca_gen == shape_gen && ca_fn == f && ca_req == cluster_ctas_opt && ca_ctas > 0)) {
+            ca_ctas = 0;
             VBD_TRY(cluster_ctas_for(fn, L, cluster_adj_smem(), &ca_ctas));
-            ca_lanes = L;
+            ca_fn = f;
             ca_gen = shape_gen;
             ca_req = cluster_ctas_opt;
         }
@@ -1623,11 +1631,12 @@ int vbd_solver_sync(vbd_solver* s) {
     DeviceScope scope(s->device);
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     if (s->status.p) {
-        unsigned long long t = 0;
-        CUDA_TRY(cudaMemcpy(&t, s->status.p + vbd::ST_TIMEOUT, sizeof(t), cudaMemcpyDeviceToHost));
-        if (t) {
+        unsigned long long t[2] = {0, 0};  // ST_TIMEOUT, ST_WALK_TIMEOUT
+        CUDA_TRY(cudaMemcpy(t, s->status.p + vbd::ST_TIMEOUT, sizeof(t), cudaMemcpyDeviceToHost));
+        if (t[0] || t[1]) {
             CUDA_TRY(cudaMemset(s->status.p + vbd::ST_TIMEOUT, 0, sizeof(t)));
-            VBD_FAIL(VBD_ERR_TIMEOUT, "a wait of the persistent kernel or the cluster walk gave up");
+            if (t[0]) VBD_FAIL(VBD_ERR_TIMEOUT, "a grid barrier of the persistent kernel gave up waiting");
+            VBD_FAIL(VBD_ERR_TIMEOUT, "an mbarrier wait of the cluster walk gave up");
         }
     }
     return VBD_OK;
