@@ -389,11 +389,11 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
  * error flag) is a fixed 32 KiB __device__ array that every GPU loading the library holds until
  * exit, so num_verts + num_tets is limited to 16,777,216 (larger sizes return
  * VBD_ERR_INVALID_ARG).  The first call on each device looks up the scratch address and must come
- * before any stream capture on that device; later calls look it up again unless their stream is
- * capturing, so a cudaDeviceReset between calls is harmless.  Calls share the scratch: calls that
- * overlap on the GPU race.  Runs on `cuda_stream` (null = default stream) and blocks the calling
- * thread until it completes; tets with ids outside [0, N) are skipped and reported as
- * VBD_ERR_INVALID_ARG. */
+ * before any stream capture on that device; later calls look it up again, so a cudaDeviceReset
+ * between calls is harmless.  Calls share the scratch: calls that overlap on the GPU race.  Runs
+ * on `cuda_stream` (null = default stream) and blocks the calling thread until it completes: it
+ * reads its error flag back and synchronises the stream, so a call cannot be captured into a CUDA
+ * graph.  Tets with ids outside [0, N) are skipped and reported as VBD_ERR_INVALID_ARG. */
 int vbd_ip_energy_noalloc(int32_t num_verts, int32_t num_tets, const float* positions, const float* inertia,
                           const float* vertex_mass, const int32_t* tets, const float* dm_inv, const float* rest_vol,
                           const float* tet_mu, const float* tet_lambda, float h, double* out, void* cuda_stream);
