@@ -158,3 +158,23 @@ def test_beam_autotune_with_cluster_candidates_completes(gpu_device):
     s.sync()
     assert s.status() == (0, False)
     s.close()
+
+
+def test_cluster_forward_with_launch_per_colour_adjoint(gpu_device):
+    """4,096 vertices: the forward walk fits (48 B per vertex) but the adjoint walk (64 B) does not,
+    so the backward recomputes through the cluster walk and sweeps the adjoint colour by colour;
+    the gradients still equal the launch-per-colour path's."""
+    m = meshgen.jittered_block(15, 15, 15, seed=5, per_tet_sigma=0.2, E=5e4)
+    assert m.num_verts == 4096
+    W = np.random.default_rng(5).normal(size=(m.num_verts, 3))
+    grads = []
+    for walk in (0, 2):
+        s = build_solver(m, lanes=8, layout=4)
+        s.set_option(_capi.OPT_PERSISTENT, walk)
+        s.record(2)
+        for _ in range(3):
+            s.step(1 / 60, 20, (0.0, -9.8, 0.0), True, 0.9)
+        grads.append(s.backward(W, None, 30, 0.9))
+        s.close()
+    for a, b in zip(grads[0], grads[1]):
+        np.testing.assert_array_equal(a, b)
