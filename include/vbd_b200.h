@@ -300,7 +300,7 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *                        (at least 4) and evaluate no energy history
  *   VBD_OPT_CLUSTER_CTAS: CTAs of the cluster walk, 1-16; 0 (default) = enough 256-thread
  *                        CTAs to sweep the largest colour in one round, at most 16.  Reading it
- *                        back after a cluster step gives the count in use
+ *                        back gives the set count, or the automatic count for the current lanes
  *   VBD_OPT_ADJOINT_ALTERNATE: 1 = adjoint sweeps alternate the colour order (a forward and a
  *                        backward sweep form one symmetric Gauss-Seidel pair)
  *   VBD_OPT_SEMANTICS:   0 = the CPU solver's (VBDsolver, VBD.cpp:114-256): Neo-Hookean element,
@@ -372,10 +372,12 @@ int vbd_solver_get_colour_lanes(vbd_solver* s, int32_t num_colours, int32_t* lan
  *      steps) against drift;
  *   4. the persistent colour-walking kernel (VBD_OPT_PERSISTENT 1) against the captured graph,
  *      then, where the mesh fits, the cluster walk (VBD_OPT_PERSISTENT 2) at 4, 8, 16 and 32
- *      threads per vertex with record layouts 3 and 4.
+ *      threads per vertex with record layouts 3 and 4, and, when it wins, its CTA count
+ *      (VBD_OPT_CLUSTER_CTAS) at about 1/2, 3/4 and 3/2 of the automatic count and at 16.
  * Phases 2-4 replace the choice only when faster by more than 1%.  chosen (may be null) receives 5
  * ints: lanes, layout, prefetch, pdl, block; the rest of the choice is read back with
- * vbd_solver_get_option (VBD_OPT_RECORD_CACHE, VBD_OPT_PERSISTENT) and vbd_solver_get_colour_lanes. */
+ * vbd_solver_get_option (VBD_OPT_RECORD_CACHE, VBD_OPT_PERSISTENT, VBD_OPT_CLUSTER_CTAS) and
+ * vbd_solver_get_colour_lanes. */
 int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t repeats, int32_t* chosen);
 
 /* Allocation-free incremental potential.  No counterpart in the reference: it exists for callers

@@ -597,14 +597,19 @@ struct vbd_solver {
 
     // CTAs of the cluster walk: enough 256-thread CTAs for the largest colour in one round, at most
     // 16, fewer when the device cannot hold a cluster of that size.
-    template <class Params>
-    int cluster_ctas_for(void (*fn)(Params), int L, size_t smem, int* out) {
+    // Enough CTAs of the cluster walk to sweep the largest colour at L lanes in one round, at most 16.
+    int cluster_auto_ctas(int L) const {
         int maxcol = 1;
         for (int c = 0; c < C; ++c) maxcol = std::max(maxcol, cstart[c + 1] - cstart[c]);
         const long long need = (long long)maxcol * L;
         const int block = vbd::kClusterMaxBlock;
-        int ctas = cluster_ctas_opt > 0 ? cluster_ctas_opt : (int)std::min<long long>(16, (need + block - 1) / block);
-        ctas = std::max(ctas, 1);
+        return (int)std::max<long long>(1, std::min<long long>(16, (need + block - 1) / block));
+    }
+
+    template <class Params>
+    int cluster_ctas_for(void (*fn)(Params), int L, size_t smem, int* out) {
+        const int block = vbd::kClusterMaxBlock;
+        int ctas = cluster_ctas_opt > 0 ? cluster_ctas_opt : cluster_auto_ctas(L);
         CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
         CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeNonPortableClusterSizeAllowed,
@@ -1815,7 +1820,10 @@ int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value) {
         case VBD_OPT_PDL: *value = s->pdl; return VBD_OK;
         case VBD_OPT_BLOCK: *value = s->block; return VBD_OK;
         case VBD_OPT_PERSISTENT: *value = s->persistent; return VBD_OK;
-        case VBD_OPT_CLUSTER_CTAS: *value = s->persistent == 2 && s->cl_ctas > 0 ? s->cl_ctas : s->cluster_ctas_opt; return VBD_OK;
+        case VBD_OPT_CLUSTER_CTAS:
+            *value = s->cluster_ctas_opt > 0 || !s->ready ? s->cluster_ctas_opt
+                                                           : s->cluster_auto_ctas(s->lanes < 4 ? 4 : s->lanes);
+            return VBD_OK;
         case VBD_OPT_SEMANTICS: *value = s->semantics; return VBD_OK;
         case VBD_OPT_L2_PREFETCH: *value = s->l2_prefetch; return VBD_OK;
         case VBD_OPT_ADJOINT_ALTERNATE: *value = s->adj_alternate; return VBD_OK;
@@ -1902,6 +1910,7 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
     struct Cand {
         int lanes, layout, prefetch, pdl, block, persistent, cache, persist;
         std::vector<int> colour_lanes;  // empty = `lanes` for every colour
+        int ctas = 0;                   // CTAs of the cluster walk (0 = automatic)
     };
     const float g[3] = {0.f, 0.f, 0.f};
     cudaEvent_t e0, e1;
@@ -1916,6 +1925,7 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
         s->record_cache = c.cache;
         s->persist_mb = c.persist;
         s->colour_lanes = c.colour_lanes;
+        s->cluster_ctas_opt = c.ctas;
         if (s->layout != c.layout) {
             s->layout = c.layout;
             return s->repack_stream();
@@ -1947,7 +1957,7 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
         {8, 0, 1, 1, 128}, {4, 0, 1, 1, 128},
     };
     Cand best{s->lanes,      s->layout,       s->eff_prefetch(), s->pdl,          s->block,
-              s->persistent, s->record_cache, s->persist_mb,     s->colour_lanes};
+              s->persistent, s->record_cache, s->persist_mb,     s->colour_lanes, s->cluster_ctas_opt};
     float best_ms = 1e30f;
     const int init_persist = s->persist_mb;  // the init-time record policy, for the factored candidates
     s->prefetch_auto = false;
@@ -2060,6 +2070,19 @@ int vbd_solver_autotune(vbd_solver* s, float dt, int32_t iterations, int32_t rep
                     if ((rc = try_cand(k))) break;
                 }
                 if (rc) break;
+            }
+            // the chosen walk's CTA count around the automatic one (fewer CTAs send fewer copies of
+            // each update; more take fewer rounds)
+            if (!rc && best.persistent == 2 && best.ctas == 0) {
+                const int a = s->cluster_auto_ctas(best.lanes < 4 ? 4 : best.lanes);
+                const Cand walk = best;
+                for (int n : {a / 2, (3 * a) / 4, a + (a + 1) / 2, 16}) {
+                    n = std::min(16, std::max(1, n));
+                    if (n == a) continue;
+                    Cand k = walk;
+                    k.ctas = n;
+                    if ((rc = try_cand(k))) break;
+                }
             }
         }
     }

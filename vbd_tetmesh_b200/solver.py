@@ -270,6 +270,8 @@ class GPUSolver:
         res["record_cache"] = self.get_option(_capi.OPT_RECORD_CACHE)
         res["persistent"] = self.get_option(_capi.OPT_PERSISTENT)
         res["colour_lanes"] = self.get_colour_lanes().tolist()
+        if res["persistent"] == 2:
+            res["cluster_ctas"] = self.get_option(_capi.OPT_CLUSTER_CTAS)
         return res
 
     def kernel_launches(self) -> int:
