@@ -36,59 +36,85 @@ def _oracle(m, steps, st, precision, x0=None, v0=None):
                        mode=po.CLOSED, threads=po.max_threads(), x0=x0, v0=v0)
 
 
-def _check_chain(name, m, st, solver, ip_f64_tol_10=None):
-    """Steps the solver and the FP32 / FP64 oracles 1 and then 9 more steps (the oracle chained
-    through its own state, which equals a direct 10-step run) and checks both checkpoints.  With
-    ip_f64_tol_10 the 10-step energy is checked against FP64 within that relative bound (the FP32
-    noise floor of the configuration) instead of 1e-5 against FP32."""
+def _check_chain(name, m, st, solvers, ip_f64_tol_10=None):
+    """Steps the solvers (a solver, or a dict of labelled solvers that share the oracle runs) and
+    the FP32 / FP64 oracles 1 and then 9 more steps (the oracle chained through its own state,
+    which equals a direct 10-step run) and checks both checkpoints.  With ip_f64_tol_10 the 10-step
+    energy is checked against FP64 within that relative bound (the FP32 noise floor of the
+    configuration) instead of 1e-5 against FP32."""
+    if not isinstance(solvers, dict):
+        solvers = {"": solvers}
     o32 = o64 = None
     done = 0
     for steps in (1, 10):
-        for _ in range(steps - done):
-            solver.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])
-        solver.sync()
-        x = solver.get_positions()
-        ip = solver.energy(0, st["dt"])
+        results = {}
+        for label, solver in solvers.items():
+            for _ in range(steps - done):
+                solver.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])
+            solver.sync()
+            results[label] = (solver.get_positions(), solver.energy(0, st["dt"]))
         o32 = _oracle(m, steps - done, st, 32, None if o32 is None else o32["x"], None if o32 is None else o32["v"])
         o64 = _oracle(m, steps - done, st, 64, None if o64 is None else o64["x"], None if o64 is None else o64["v"])
         done = steps
-        e32, e64, n64 = rel_err(x, o32["x"], m), rel_err(x, o64["x"], m), rel_err(o32["x"], o64["x"], m)
-        ip32, ip64 = o32["ip"][-1], o64["ip"][-1]
-        print(f"{name} {steps} steps: |gpu - oracle32|/diag {e32:.3e}, |gpu - oracle64|/diag {e64:.3e} "
-              f"(oracle32 vs 64: {n64:.3e}); IP gpu {ip:.9g} vs32 {abs(ip - ip32) / abs(ip32):.2e} "
-              f"vs64 {abs(ip - ip64) / abs(ip64):.2e} (oracle32 vs64 {abs(ip32 - ip64) / abs(ip64):.2e})")
-        assert e32 < POS_TOL
-        assert e64 < POS_TOL
-        if steps == 10 and ip_f64_tol_10 is not None:
-            assert abs(ip - ip64) <= ip_f64_tol_10 * abs(ip64)
-            assert abs(ip32 - ip64) <= ip_f64_tol_10 * abs(ip64)
-        else:
-            assert abs(ip - ip32) <= IP_TOL * abs(ip32)
-    sing, nonf = solver.status()
-    assert sing == 0 and not nonf
+        for label, (x, ip) in results.items():
+            e32, e64, n64 = rel_err(x, o32["x"], m), rel_err(x, o64["x"], m), rel_err(o32["x"], o64["x"], m)
+            ip32, ip64 = o32["ip"][-1], o64["ip"][-1]
+            print(f"{name}{' ' + label if label else ''} {steps} steps: |gpu - oracle32|/diag {e32:.3e}, "
+                  f"|gpu - oracle64|/diag {e64:.3e} (oracle32 vs 64: {n64:.3e}); IP gpu {ip:.9g} "
+                  f"vs32 {abs(ip - ip32) / abs(ip32):.2e} vs64 {abs(ip - ip64) / abs(ip64):.2e} "
+                  f"(oracle32 vs64 {abs(ip32 - ip64) / abs(ip64):.2e})")
+            assert e32 < POS_TOL
+            assert e64 < POS_TOL
+            if steps == 10 and ip_f64_tol_10 is not None:
+                assert abs(ip - ip64) <= ip_f64_tol_10 * abs(ip64)
+                assert abs(ip32 - ip64) <= ip_f64_tol_10 * abs(ip64)
+            else:
+                assert abs(ip - ip32) <= IP_TOL * abs(ip32)
+    for solver in solvers.values():
+        sing, nonf = solver.status()
+        assert sing == 0 and not nonf
+
+
+# The cube's launch shape as the autotuner picks it on this pool's B200s (bench.py tunes before
+# timing): packed factored records, threads per vertex 4,8,4,8,4,4,8,8 by colour, each lane's first
+# three records loaded before the dependency wait, evict-first records with a 32 MB evict-last prefix.
+CUBE64_TUNED = {"colour_lanes": [4, 8, 4, 8, 4, 4, 8, 8], _capi.OPT_PREFETCH: 2, _capi.OPT_RECORD_CACHE: 1,
+                _capi.OPT_RECORD_PERSIST_MB: 32}
 
 
 def test_cube64_matches_oracle(gpu_device):
-    """The benched workload itself, with the bench's launch shape (chosen at init: packed factored
-    records, 8 lanes, deep record prefetch)."""
+    """The benched workload itself, with the launch shape init picks (packed factored records, 8
+    lanes, deep record prefetch) and with the bench's autotuned shape (CUBE64_TUNED), against the
+    same oracle runs."""
     m = meshgen.cube(64)
     assert (m.num_verts, m.num_tets) == (274625, 1572864)
     st = meshgen.CUBE_SETTINGS
-    s = build_solver(m, device=gpu_device)
+    init = build_solver(m, device=gpu_device)
+    tuned = build_solver(m, device=gpu_device)
     try:
-        _check_chain("cube64", m, st, s, ip_f64_tol_10=CUBE64_IP_TOL_F64)
+        tuned.set_colour_lanes(CUBE64_TUNED["colour_lanes"])
+        for k, v in CUBE64_TUNED.items():
+            if k != "colour_lanes":
+                tuned.set_option(k, v)
+        _check_chain("cube64", m, st, {"init shape": init, "tuned shape": tuned}, ip_f64_tol_10=CUBE64_IP_TOL_F64)
     finally:
-        s.close()
+        init.close()
+        tuned.close()
 
 
 def test_diff_beam_forward_matches_oracle(gpu_device):
+    """The differentiated beam with the captured graph (init's shape) and with the cluster walk the
+    bench's autotuner picks for it (8 lanes, stored-det records), against the same oracle runs."""
     m, _, _ = meshgen.diff_beam()
     st = meshgen.DIFF_SETTINGS
-    s = build_solver(m, device=gpu_device)
+    graph = build_solver(m, device=gpu_device)
+    walk = build_solver(m, device=gpu_device, lanes=8, layout=3)
     try:
-        _check_chain("diff_beam", m, st, s)
+        walk.set_option(_capi.OPT_PERSISTENT, 2)
+        _check_chain("diff_beam", m, st, {"graph": graph, "cluster walk": walk})
     finally:
-        s.close()
+        graph.close()
+        walk.close()
 
 
 # The batched configuration's stated sizes; the sample is seeded.
