@@ -629,7 +629,7 @@ def bench_adjoint(local, stream, autotune=True):
     }
 
 
-def bench_material_id(local, stream):
+def bench_material_id(local, stream, autotune=True):
     """Batched material identification: 64 beams (Lx U{8..40}, Ly = Lz U{3..8}), hidden (E, nu) as the
     batched configuration, targets from a 20-step forward under gravity; per-mesh gradients of
     (log E, nu) from one batched forward + adjoint vs central finite differences of the batched
@@ -643,6 +643,8 @@ def bench_material_id(local, stream):
         meshes, hidden = mid.beams(64)
         prob = mid.Problem.create(meshes, device=local, stream=stream.cuda_stream)
         targets = prob.forward(np.log(hidden[:, 0]), hidden[:, 1])
+        st = mid.Settings()
+        tuned = prob.solver.autotune(st.dt, iterations=st.iterations, repeats=2) if autotune else None
         logE0 = np.full(len(meshes), np.log(1e5))
         nu0 = np.full(len(meshes), 0.3)
         t0 = time.perf_counter()
@@ -659,8 +661,8 @@ def bench_material_id(local, stream):
     relE = np.abs(np.exp(logE) / hidden[:, 0] - 1.0)
     dnu = np.abs(nu - hidden[:, 1])
     q = lambda a: {"median": float(np.median(a)), "p90": float(np.percentile(a, 90)), "max": float(np.max(a))}  # noqa: E731
-    st = mid.Settings()
     return {
+        "autotuned": tuned,
         "workload": f"{len(meshes)} beams, {prob.batch.num_verts} vertices, {prob.batch.num_tets} tets, "
                     f"{st.steps} steps x {st.iterations} iterations, adjoint {st.adjoint_iterations} sweeps, "
                     "all meshes in one solver",
@@ -888,7 +890,7 @@ def main():
         result["beam"] = bench_beam(local, stream, not args.no_autotune)
         result["adjoint"] = bench_adjoint(local, stream, not args.no_autotune)
     if not args.no_material_id and rank == 0:
-        result["material_id"] = bench_material_id(local, stream)
+        result["material_id"] = bench_material_id(local, stream, not args.no_autotune)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu_value, cores, total, kind, what = cpu_reference(mesh, 3, warmup=1)
