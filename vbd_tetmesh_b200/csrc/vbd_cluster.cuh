@@ -46,11 +46,11 @@ __device__ __forceinline__ unsigned cluster_size() {
     return r;
 }
 
-// Cluster-wide barrier, split so that independent loads can be issued between the two halves.  The
-// release / acquire pair orders every shared (local and distributed) and global memory access
-// before the arrive against those after the wait, across the cluster.
-// Every thread of the cluster takes the same barriers in the same order (the loops are uniform), and
-// each warp is reconverged first, so the warp-aligned forms apply.
+// Cluster-wide barrier (taken once before the first colour and once before the walk ends), split so
+// that independent loads can be issued between the two halves.  The release / acquire pair orders
+// every shared (local and distributed) and global memory access before the arrive against those
+// after the wait, across the cluster.  Every thread of the cluster takes it, each warp reconverged
+// first, so the warp-aligned forms apply.
 __device__ __forceinline__ void cluster_arrive() {
     __syncwarp();
     asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
@@ -118,8 +118,8 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigne
     return done;
 }
 
-// What a vertex group needs before it can sweep its vertex, loaded ahead of the barrier: the
-// lane's first kClusterAhead element records, and (first lane) the inertial target and the
+// What a vertex group needs before it can sweep its vertex, loaded while the previous colour is
+// still arriving: the lane's first kClusterAhead element records, and (first lane) the inertial target and the
 // position before the previous sweep.  Element data and y do not change during the sweeps; the
 // pre-sweep position is kept in this CTA's shared memory (pp, indexed by vertex) and written only
 // by this same thread.
