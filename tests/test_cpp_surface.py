@@ -1,7 +1,6 @@
 """The C++ drop-in surface (include/vbd/*.h) compiles, and the reference's own driver compiles and
 links against it unchanged (no GPU needed: nothing runs)."""
 import os
-import shutil
 import subprocess
 
 import pytest

@@ -11,7 +11,7 @@ import ctypes as C
 import numpy as np
 
 from . import _capi
-from ._capi import call, lib
+from ._capi import call
 
 
 def _ptr(a: np.ndarray | None):
