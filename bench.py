@@ -539,9 +539,23 @@ def bench_beam(local, stream, autotune=True):
         s.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])
         s.sync()
         launches = s.kernel_launches() - launches_before
+        persistent = s.get_option(_capi.OPT_PERSISTENT)
         path = {0: "captured CUDA graph", 1: "persistent kernel with grid barriers",
-                2: "cluster walk (one thread-block cluster, positions in distributed shared memory)"}[
-            s.get_option(_capi.OPT_PERSISTENT)]
+                2: "cluster walk (one thread-block cluster, positions in distributed shared memory)"}[persistent]
+        graph_ms = None
+        if persistent:  # the same shape through the captured graph of per-colour launches
+            s.set_option(_capi.OPT_PERSISTENT, 0)
+            s.set_positions(m.x)
+            s.set_velocities(m.v)
+            s.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])  # capture
+            s.set_positions(m.x)
+            s.set_velocities(m.v)
+            s.sync()
+            t0 = time.perf_counter()
+            for _ in range(st["steps"]):
+                s.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])
+            s.sync()
+            graph_ms = (time.perf_counter() - t0) * 1e3 / st["steps"]
         s.close()
     vi = m.num_verts * st["iterations"] * st["steps"]
     return {
@@ -552,6 +566,7 @@ def bench_beam(local, stream, autotune=True):
         "unit": "vertex-iterations/s",
         "kernel_launches_per_step": launches,
         "path": path,
+        "same_shape_captured_graph_ms_per_step": graph_ms,
         "autotuned": tuned,
         "how": "wall time around 100 vbd_solver_step calls (best of 3), positions resident on the device",
     }
@@ -572,26 +587,36 @@ def bench_adjoint(local, stream, autotune=True):
         s = build_solver(m, device=local, stream=stream.cuda_stream)
         tuned = s.autotune(st["dt"], iterations=st["iterations"], repeats=3) if autotune else None
         persistent = s.get_option(_capi.OPT_PERSISTENT)
-        res = []
-        for _ in range(3):
-            s.set_positions(m.x)
-            s.set_velocities(m.v)
-            s.record(st["checkpoint"])
-            s.sync()
-            t0 = time.perf_counter()
-            for _ in range(st["steps"]):
-                s.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])
-            s.sync()
-            tf = time.perf_counter() - t0
-            x = s.get_positions().astype(np.float64)
-            g = np.zeros((m.num_verts, 3))
-            g[tip] = 2.0 * (x[tip] - target)
-            t0 = time.perf_counter()
-            s.backward(g, None, st["adjoint_iterations"], st["adjoint_rho"])
-            tb = time.perf_counter() - t0
-            res.append((tf, tb))
+
+        def forward_backward():
+            res = []
+            for _ in range(3):
+                s.set_positions(m.x)
+                s.set_velocities(m.v)
+                s.record(st["checkpoint"])
+                s.sync()
+                t0 = time.perf_counter()
+                for _ in range(st["steps"]):
+                    s.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])
+                s.sync()
+                tf = time.perf_counter() - t0
+                x = s.get_positions().astype(np.float64)
+                g = np.zeros((m.num_verts, 3))
+                g[tip] = 2.0 * (x[tip] - target)
+                t0 = time.perf_counter()
+                s.backward(g, None, st["adjoint_iterations"], st["adjoint_rho"])
+                tb = time.perf_counter() - t0
+                res.append((tf, tb))
+            return min(res, key=lambda r: r[1])
+
+        tf, tb = forward_backward()
+        # the same shape through the captured graph of per-colour launches, for comparison
+        graph = None
+        if persistent:
+            s.set_option(_capi.OPT_PERSISTENT, 0)
+            gf, gb = forward_backward()
+            graph = {"forward_ms": gf * 1e3, "backward_ms": gb * 1e3, "backward_over_forward": gb / gf}
         s.close()
-    tf, tb = min(res, key=lambda r: r[1])
     # Algorithmic bytes of the backward pass: the recomputed forward sweeps of the older segments
     # (the newest segment's states are kept) at the forward's 60 B per incidence + 96 B per swept
     # vertex, and the adjoint sweeps at 68 B per incidence (the record plus per-tet mu, lambda) +
@@ -614,6 +639,7 @@ def bench_adjoint(local, stream, autotune=True):
         "adjoint_rho": st["adjoint_rho"],
         "autotuned": tuned,
         "forward_path": {0: "captured CUDA graph", 1: "persistent kernel", 2: "cluster walk"}[persistent],
+        "same_shape_captured_graph": graph,
         "accuracy": "checked in tests/test_gpu_adjoint.py: <= 1e-3 relative vs the FP64 implicit adjoint",
         "roofline": {
             "bound": "latency: 2,673 vertices give under 1% of the GPU's resident threads work",
