@@ -697,10 +697,11 @@ def bench_material_id(local, stream, autotune=True):
         "grad_vs_fd_rel_nu": q(eN),
         "grad_fd": "central differences of the batched FP32 GPU forward, step 1e-3 (FP32 noise dominates at 1e-4); "
                    "checked against FP64 finite differences at converged iterations in tests/test_gpu_material_id.py",
-        "optimizer": "per-mesh trust-region quasi-Newton (2x2 BFGS on log E, nu/0.1); every iteration is one "
-                     "batched forward + adjoint of all meshes; a mesh whose trials fail twice in a row (the forward "
-                     "far from converged, so the implicit gradient misleads) takes central finite differences of the "
-                     "batched forward from then on",
+        "optimizer": "per-mesh trust-region quasi-Newton (2x2 BFGS on log E, nu/0.1) with E kept in [5e3, 2e6] "
+                     "(the configuration draws it from [1e4, 1e6]); every iteration is one batched forward + adjoint "
+                     "of all meshes; a mesh whose trials fail twice in a row, or whose last 5 accepted steps together "
+                     "lowered its loss by less than 10% (the forward far from converged, so the implicit gradient "
+                     "misleads), takes central finite differences of the batched forward from then on",
         "meshes_on_finite_differences": id_info["fd_meshes"],
         "batched_forward_adjoints": id_info["forward_backwards"],
         "batched_forwards": id_info["forwards"],

@@ -128,8 +128,8 @@ class Problem:
 NU_SCALE = 0.1  # nu is optimised as nu / NU_SCALE, so both coordinates move on similar scales
 
 
-def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), radius0=(1.0, 0.5), armijo=1e-4,
-             fd_after=2, fd_step=1e-3, converged=1e-7):
+def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), E_bounds=(5e3, 2e6), radius0=(1.0, 0.5),
+             armijo=1e-4, fd_after=2, fd_step=1e-3, converged=1e-7, stall_window=5, stall_gain=0.1, trace=None):
     """Per-mesh trust-region quasi-Newton descent on z = (log E, nu / NU_SCALE).
 
     Every mesh keeps its own 2x2 BFGS inverse-Hessian estimate and its own trust radius (per
@@ -141,14 +141,20 @@ def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), rad
     rejected fd_after times in a row, while its loss is still above `converged` times its initial
     loss (below that, rejections come from FP32 noise in the loss), therefore takes central finite
     differences of the batched forward (step fd_step) as its gradient from then on; those forwards
-    are run only while some mesh needs them.  nu is kept inside nu_bounds.
+    are run only while some mesh needs them.  The same switch happens when a mesh's last
+    stall_window accepted steps together lowered its loss by less than stall_gain of it: steps that
+    are accepted but barely help also mark a gradient that does not point downhill.  nu is kept
+    inside nu_bounds and E inside E_bounds (the batched configuration draws E from [1e4, 1e6];
+    beyond it a very stiff beam barely moves, and the flat loss there holds a descent back).
 
     Returns (logE, nu, history of the total loss at the accepted points, per-mesh final losses, info)
-    with info = dict(fd_meshes, forwards, forward_backwards)."""
+    with info = dict(fd_meshes, forwards, forward_backwards).  A list passed as `trace` receives,
+    per outer iteration, a dict of per-mesh arrays: z, loss, trial loss, accepted, radius, use_fd."""
     M = len(problem.batch.meshes)
     z = np.stack([np.asarray(logE0, np.float64), np.asarray(nu0, np.float64) / NU_SCALE], axis=1)
-    lo = np.array([-np.inf, nu_bounds[0] / NU_SCALE])
-    hi = np.array([np.inf, nu_bounds[1] / NU_SCALE])
+    lo = np.array([np.log(E_bounds[0]), nu_bounds[0] / NU_SCALE])
+    hi = np.array([np.log(E_bounds[1]), nu_bounds[1] / NU_SCALE])
+    z = np.clip(z, lo, hi)
     counts = {"forwards": 0, "forward_backwards": 0}
 
     def evaluate(zz):
@@ -175,6 +181,7 @@ def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), rad
     Hinv = np.zeros((M, 2, 2))
     rejects = np.zeros(M, int)
     use_fd = np.zeros(M, bool)
+    accepted_losses = [[float(L[m])] for m in range(M)]  # loss after each accepted step
     zp, gp = z.copy(), g.copy()          # a finite-difference mesh's previous point and gradient
     have_prev = np.zeros(M, bool)
 
@@ -225,7 +232,15 @@ def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), rad
             if not use_fd[m]:
                 bfgs(m, trial[m] - z[m], gt[m] - g[m])
             z[m], L[m], g[m] = trial[m], Lt[m], gt[m]
+            hist_m = accepted_losses[m]
+            hist_m.append(float(Lt[m]))
+            if (not use_fd[m] and len(hist_m) > stall_window and L[m] > converged * L0[m]
+                    and hist_m[-1 - stall_window] - hist_m[-1] < stall_gain * hist_m[-1 - stall_window]):
+                use_fd[m] = True
         hist.append(float(L.sum()))
+        if trace is not None:
+            trace.append(dict(z=z.copy(), loss=L.copy(), trial_loss=np.asarray(Lt).copy(), accepted=ok.copy(),
+                              radius=radius.copy(), use_fd=use_fd.copy()))
     info = dict(fd_meshes=int(use_fd.sum()), **counts)
     return z[:, 0], z[:, 1] * NU_SCALE, hist, L, info
 
