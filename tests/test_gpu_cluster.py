@@ -178,3 +178,43 @@ def test_cluster_forward_with_launch_per_colour_adjoint(gpu_device):
         s.close()
     for a, b in zip(grads[0], grads[1]):
         np.testing.assert_array_equal(a, b)
+
+
+def test_cluster_walk_with_energy_history_runs_separate_launches(gpu_device):
+    """A step that must append VBDsolver's energy history runs as separate launches even with the
+    cluster walk selected, and its positions and energies equal the graph path's."""
+    m = meshgen.beam()
+    st = meshgen.BEAM_SETTINGS
+    out = []
+    for walk in (0, 2):
+        s = build_solver(m, lanes=16, layout=3)
+        s.set_option(_capi.OPT_PERSISTENT, walk)
+        s.set_option(_capi.OPT_ENERGY_EVERY, 10)
+        for _ in range(3):
+            s.step(st["dt"], st["iterations"], st["gravity"], True, st["rho"])
+        out.append((s.get_positions(), s.energy_history()))
+        s.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    assert len(out[1][1]) == 3 * 2
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+
+
+def test_cluster_walk_refuses_a_reinitialised_mesh_that_does_not_fit(gpu_device):
+    from vbd_tetmesh_b200 import color_vertices, mesh_mass, precompute_tets
+
+    s = build_solver(small_block(seed=2), layout=4)
+    s.set_option(_capi.OPT_PERSISTENT, 2)
+    s.step(1 / 60, 5, (0.0, -9.8, 0.0), True, 0.9)
+    big = meshgen.cube(24)
+    _, offs, verts = color_vertices(big.num_verts, big.tets)
+    mass, _ = mesh_mass(big.rest, big.tets, big.density)
+    dminv, v0 = precompute_tets(big.rest, big.tets)
+    s.init_from_cpu(big.x, mass, big.fixed, big.tets, offs, verts, dminv, v0, big.mu, big.lam)
+    with pytest.raises(_capi.VBDError) as e:
+        s.step(1 / 120, 5, (0.0, -9.8, 0.0), True, 0.9)
+    assert e.value.code == 1  # VBD_ERR_INVALID_ARG: does not fit
+    s.set_option(_capi.OPT_PERSISTENT, 0)
+    s.step(1 / 120, 5, (0.0, -9.8, 0.0), True, 0.9)
+    s.sync()
+    assert np.all(np.isfinite(s.get_positions()))
+    s.close()
