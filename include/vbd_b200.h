@@ -301,6 +301,11 @@ int vbd_solver_status(vbd_solver* s, int64_t* singular_skips, int32_t* nonfinite
  *   VBD_OPT_CLUSTER_CTAS: CTAs of the cluster walk, 1-16; 0 (default) = enough 256-thread
  *                        CTAs to sweep the largest colour in one round, at most 16.  Reading it
  *                        back gives the set count, or the automatic count for the current lanes
+ *   VBD_OPT_CLUSTER_RESIDENT: 1 (default) = the cluster walk copies, once per sub-step, the element
+ *                        records, inertial targets and incidence spans of the vertices each CTA
+ *                        sweeps into that CTA's shared memory when they fit beside the positions,
+ *                        so no colour waits on L2 for them; 0 = they are read from L2 each colour.
+ *                        Same results either way
  *   VBD_OPT_ADJOINT_ALTERNATE: 1 = adjoint sweeps alternate the colour order (a forward and a
  *                        backward sweep form one symmetric Gauss-Seidel pair)
  *   VBD_OPT_SEMANTICS:   0 = the CPU solver's (VBDsolver, VBD.cpp:114-256): Neo-Hookean element,
@@ -345,7 +350,8 @@ typedef enum vbd_option {
     VBD_OPT_RECORD_CACHE = 11,
     VBD_OPT_RECORD_PERSIST_MB = 12,
     VBD_OPT_ENERGY_EVERY = 13,
-    VBD_OPT_CLUSTER_CTAS = 14
+    VBD_OPT_CLUSTER_CTAS = 14,
+    VBD_OPT_CLUSTER_RESIDENT = 15
 } vbd_option;
 int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value);
 int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value);

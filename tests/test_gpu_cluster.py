@@ -218,3 +218,27 @@ def test_cluster_walk_refuses_a_reinitialised_mesh_that_does_not_fit(gpu_device)
     s.sync()
     assert np.all(np.isfinite(s.get_positions()))
     s.close()
+
+
+@pytest.mark.parametrize("case,lanes,layout,ctas", [("beam", 16, 3, 0), ("beam", 32, 4, 0), ("diff", 8, 4, 16),
+                                                    ("block", 4, 3, 3), ("diff", 16, 4, 1)])
+def test_resident_records_change_no_bits(gpu_device, case, lanes, layout, ctas):
+    """VBD_OPT_CLUSTER_RESIDENT 1 keeps each CTA's element records, inertial targets and spans in its
+    shared memory where they fit (the differentiated beam at 8 lanes only with 16 CTAs; with one
+    CTA they do not fit and the walk reads them from L2); 0 always reads them from L2.  Both equal
+    the captured graph bit for bit."""
+    if case == "beam":
+        m, st = meshgen.beam(), meshgen.BEAM_SETTINGS
+    elif case == "diff":
+        m, st = meshgen.diff_beam()[0], meshgen.DIFF_SETTINGS
+    else:
+        m, st = small_block(seed=9, dims=(9, 5, 4)), dict(dt=1 / 60, iterations=15, rho=0.9, gravity=(0.0, -9.8, 0.0))
+    args = (m, 3, st["dt"], st["iterations"], st["gravity"], True, st["rho"])
+    graph = gpu_simulate(*args, lanes=lanes, layout=layout)
+    for resident in (1, 0):
+        w = gpu_simulate(*args, lanes=lanes, layout=layout,
+                         options={_capi.OPT_PERSISTENT: 2, _capi.OPT_CLUSTER_CTAS: ctas,
+                                  _capi.OPT_CLUSTER_RESIDENT: resident})
+        np.testing.assert_array_equal(graph["x"], w["x"])
+        np.testing.assert_array_equal(graph["v"], w["v"])
+        assert w["singular"] == 0 and not w["nonfinite"]

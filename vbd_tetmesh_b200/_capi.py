@@ -43,6 +43,7 @@ OPT_RECORD_CACHE = 11
 OPT_RECORD_PERSIST_MB = 12
 OPT_ENERGY_EVERY = 13
 OPT_CLUSTER_CTAS = 14
+OPT_CLUSTER_RESIDENT = 15
 SEMANTICS_VBDSOLVER = 0
 SEMANTICS_GPU_WRAPPER = 1
 

@@ -329,6 +329,242 @@ __global__ void __launch_bounds__(kClusterMaxBlock, 1) k_cluster_walk(PersistPar
     }
 }
 
+// ---- The cluster walk with resident element data ------------------------------------------------
+//
+// In the walk above, the CTA that finishes a colour last has no wait in which its next colour's
+// element records (from L2) could arrive, so their latency sits on the critical path every colour
+// (long-scoreboard stalls lead its profile).  Where they fit, each CTA instead copies, once per
+// sub-step, the records, inertial targets and incidence spans of exactly the vertices its groups
+// sweep into shared memory.  Group g of CTA k sweeps, in round r of colour c, vertex
+// vb_c + r * groups + k * gpc + (g - k * gpc): the CTA's vertices of one (colour, round) slice are
+// one contiguous run, and so are their incidences, so a slice is one contiguous copy.  Same
+// arithmetic and record order as the walk above, hence the same bits.
+
+// Byte offsets of the regions of the resident walk's dynamic shared memory (16-byte aligned).
+struct SrecLayout {
+    unsigned long long x, rec, mat, y, pp, span, tab, rows, total;
+};
+__host__ __device__ inline unsigned long long srec_align(unsigned long long b) { return (b + 15ull) & ~15ull; }
+__host__ __device__ inline SrecLayout srec_layout(int n, int records, int owned, int slices, int ncol, int layout) {
+    SrecLayout L;
+    const unsigned long long words = layout == 4 ? 2 : 3;  // int4 per record in the record stream
+    L.x = 0;
+    L.rec = srec_align(L.x + 32ull * (unsigned long long)n);
+    L.mat = srec_align(L.rec + 16ull * words * (unsigned long long)records);
+    L.y = srec_align(L.mat + (layout == 4 ? 8ull * (unsigned long long)records : 0ull));
+    L.pp = srec_align(L.y + 16ull * (unsigned long long)owned);
+    L.span = srec_align(L.pp + 16ull * (unsigned long long)owned);
+    L.tab = srec_align(L.span + 8ull * (unsigned long long)owned);
+    L.rows = srec_align(L.tab + 16ull * (unsigned long long)slices);
+    L.total = srec_align(L.rows + 4ull * (unsigned long long)(ncol + 1));
+    return L;
+}
+
+// A record from shared memory, in the layouts' raw form.
+template <int LAYOUT> struct SRec;
+template <> struct SRec<4> {
+    __device__ __forceinline__ static FactRaw4 get(const int4* cs, const float2* cm, int j) {
+        FactRaw4 r;
+        r.w0 = cs[2 * j];
+        r.w1 = reinterpret_cast<const float4*>(cs)[2 * j + 1];
+        r.m = cm[j];
+        return r;
+    }
+};
+template <> struct SRec<3> {
+    __device__ __forceinline__ static FactRaw3 get(const int4* cs, const float2*, int j) {
+        FactRaw3 r;
+        r.w0 = cs[3 * j];
+        r.w1 = reinterpret_cast<const float4*>(cs)[3 * j + 1];
+        r.w2 = reinterpret_cast<const float4*>(cs)[3 * j + 2];
+        return r;
+    }
+};
+
+// One vertex of a colour sweep with its CTA-local data at slot lv (records [span.x, span.y) of the
+// CTA's resident records).  All lanes of the warp call it.
+template <int LANES, int LAYOUT>
+__device__ __forceinline__ void cluster_vertex_srec(const PersistParams& p, const float4* xs, const float4* xb,
+                                                    const int4* cs, const float2* cm, const float4* ys, float4* pps,
+                                                    const int2* spans, unsigned bar, int v, int lv, bool active,
+                                                    int lane, int lane_w, unsigned csize, bool blend, float omega) {
+    const float4 xi = active ? xs[v] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int2 sp = active ? spans[lv] : make_int2(0, 0);
+    Acc acc;
+    acc.zero();
+    for (int j = sp.x + lane; j < sp.y; j += LANES)
+        Elem<LAYOUT>::template contrib<true>(SRec<LAYOUT>::get(cs, cm, j), v, xi, xs, acc);
+    group_reduce<LANES>(acc);
+    float4 xn = xi, xa = xi;
+    if (active && lane == 0) {
+        xn = block_solve(acc, xi, ys[lv], p.sw.dtsr, p.sw.status);
+        if (blend) xa = cheb_blend(xn, pps[lv], omega);
+        if (p.sw.keep_pp) pps[lv] = xi;
+    }
+    const int leader = lane_w & ~(LANES - 1);
+    xn.x = __shfl_sync(0xffffffffu, xn.x, leader);
+    xn.y = __shfl_sync(0xffffffffu, xn.y, leader);
+    xn.z = __shfl_sync(0xffffffffu, xn.z, leader);
+    xn.w = __shfl_sync(0xffffffffu, xn.w, leader);
+    if (blend) {
+        xa.x = __shfl_sync(0xffffffffu, xa.x, leader);
+        xa.y = __shfl_sync(0xffffffffu, xa.y, leader);
+        xa.z = __shfl_sync(0xffffffffu, xa.z, leader);
+        xa.w = __shfl_sync(0xffffffffu, xa.w, leader);
+    }
+    if (!active) return;
+    const unsigned sn = (unsigned)__cvta_generic_to_shared(xs + v);
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(xb + v);
+    for (unsigned r = (unsigned)lane; r < csize; r += LANES) {
+        const unsigned rb = cluster_map(bar, r);
+        st_async(cluster_map(sn, r), xn, rb);
+        if (blend) st_async(cluster_map(sa, r), xa, rb);
+    }
+}
+
+// The walk above with each CTA's element records, inertial targets and pre-sweep positions resident
+// in its shared memory (layout srec_layout; the host sizes it from the same slice plan).
+template <int LANES, int LAYOUT>
+__global__ void __launch_bounds__(kClusterMaxBlock, 1) k_cluster_walk_srec(PersistParams p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long mbar[2];
+    __shared__ int plan_ok;
+    const int n = p.n;
+    const SrecLayout Ly = srec_layout(n, p.srec_records, p.srec_owned, p.srec_slices, p.ncol, LAYOUT);
+    float4* sx = reinterpret_cast<float4*>(smem + Ly.x);
+    int4* cs = reinterpret_cast<int4*>(smem + Ly.rec);
+    float2* cm = reinterpret_cast<float2*>(smem + Ly.mat);
+    float4* ys = reinterpret_cast<float4*>(smem + Ly.y);
+    float4* pps = reinterpret_cast<float4*>(smem + Ly.pp);
+    int2* spans = reinterpret_cast<int2*>(smem + Ly.span);
+    int4* tab = reinterpret_cast<int4*>(smem + Ly.tab);  // per slice: first vertex, count, vertex slot, record slot
+    int* rows = reinterpret_cast<int*>(smem + Ly.rows);  // first slice of each colour
+    const unsigned csize = cluster_size();
+    const unsigned crank = cluster_rank();
+    const int tid = threadIdx.x;
+    const int gt = (int)crank * (int)blockDim.x + tid;
+    const int nthreads = (int)csize * (int)blockDim.x;
+    const int lane_w = tid & 31;
+    const int lane = LANES == 1 ? 0 : (lane_w & (LANES - 1));
+    const int grp = gt / LANES;
+    const int ngroups = nthreads / LANES;
+    const int gpc = (int)blockDim.x / LANES;  // groups per CTA
+    const int lg = tid / LANES;               // this thread's group within the CTA
+    float4* y = const_cast<float4*>(p.sw.y);
+    const unsigned bar0 = (unsigned)__cvta_generic_to_shared(&mbar[0]);
+    const unsigned total = (unsigned)max(p.iters, 0) * (unsigned)p.ncol;
+    if (tid == 0) {  // as in k_cluster_walk: colours 0 and 1 announced before the first barrier
+        mbar_init(bar0);
+        mbar_init(bar0 + 8);
+        if (total > 0) mbar_expect(bar0, walk_bytes(p, 0));
+        if (total > 1) mbar_expect(bar0 + 8, walk_bytes(p, 1));
+        fence_mbar_init();
+        // this CTA's (colour, round) slices
+        int sl = 0, vbase = 0, rbase = 0;
+        for (int c = 0; c < p.ncol; ++c) {
+            rows[c] = sl;
+            const int vb = __ldg(p.cstart + c), ve = __ldg(p.cstart + c + 1);
+            const int rounds = (ve - vb + ngroups - 1) / ngroups;
+            for (int r = 0; r < rounds; ++r, ++sl) {
+                const int vf = vb + r * ngroups + (int)crank * gpc;
+                const int cnt = max(0, min(vf + gpc, ve) - vf);
+                if (sl < p.srec_slices) tab[sl] = make_int4(vf, cnt, vbase, rbase);
+                vbase += cnt;
+                if (cnt) rbase += __ldg(p.sw.inc_off + vf + cnt) - __ldg(p.sw.inc_off + vf);
+            }
+        }
+        rows[p.ncol] = sl;
+        // the host sized the regions from the same plan; refuse rather than overrun them
+        plan_ok = sl == p.srec_slices && vbase <= p.srec_owned && rbase <= p.srec_records;
+        if (!plan_ok) atomicOr(reinterpret_cast<unsigned int*>(p.sw.status + ST_WALK_TIMEOUT), 1u);
+    }
+
+    if (p.predict)
+        for (int i = gt; i < n; i += nthreads)
+            predict_vertex(i, p.xa, p.v, p.xprev, y, p.nfree, p.h, p.hgx, p.hgy, p.hgz);
+    if (p.init_from_inertia)
+        for (int i = gt; i < n; i += nthreads) {
+            const float4 yi = y[i];
+            float4 a = p.xa[i], b = p.xb[i];
+            a.x = b.x = yi.x;
+            a.y = b.y = yi.y;
+            a.z = b.z = yi.z;
+            p.xa[i] = a;
+            p.xb[i] = b;
+        }
+    for (int i = tid; i < n; i += blockDim.x) {
+        float4 a = p.xa[i];
+        float4 b = p.xb[i];
+        if (p.init_from_inertia) {
+            const float4 yi = y[i];
+            a.x = b.x = yi.x;
+            a.y = b.y = yi.y;
+            a.z = b.z = yi.z;
+        }
+        sx[i] = a;
+        sx[n + i] = b;
+    }
+    __syncthreads();
+    const bool ok_plan = plan_ok != 0;
+    constexpr int words = LAYOUT == 4 ? 2 : 3;
+    if (ok_plan)  // the CTA's records and incidence spans, one contiguous run per slice
+        for (int sl = 0; sl < p.srec_slices; ++sl) {
+            const int4 t = tab[sl];
+            if (t.y == 0) continue;
+            const int jb = __ldg(p.sw.inc_off + t.x);
+            const int cnt = __ldg(p.sw.inc_off + t.x + t.y) - jb;
+            for (int w = tid; w < cnt * words; w += blockDim.x) cs[t.w * words + w] = __ldg(p.sw.crec + jb * words + w);
+            if constexpr (LAYOUT == 4)
+                for (int i = tid; i < cnt; i += blockDim.x) cm[t.w + i] = __ldg(p.sw.cmat + jb + i);
+            for (int i = tid; i < t.y; i += blockDim.x)
+                spans[t.z + i] = make_int2(t.w + __ldg(p.sw.inc_off + t.x + i) - jb,
+                                           t.w + __ldg(p.sw.inc_off + t.x + i + 1) - jb);
+        }
+    cluster_arrive();
+    cluster_wait();
+    if (ok_plan)  // inertial targets: the predictor's writes are visible after the barrier
+        for (int sl = 0; sl < p.srec_slices; ++sl) {
+            const int4 t = tab[sl];
+            for (int i = tid; i < t.y; i += blockDim.x) ys[t.z + i] = __ldcg(p.sw.y + t.x + i);
+        }
+    __syncthreads();
+
+    int cur = 0;
+    unsigned gc = 0;
+    bool alive = ok_plan;
+    for (int k = 0; k < p.iters && alive; ++k) {
+        const float om = __ldg(p.omega + k);
+        const bool blend = om > 1.0f;
+        const float4* xs = sx + (cur ? n : 0);
+        const float4* xb = sx + (cur ? 0 : n);
+        for (int c = 0; c < p.ncol; ++c, ++gc) {
+            const int vb = __ldg(p.cstart + c), ve = __ldg(p.cstart + c + 1);
+            const unsigned bar = bar0 + 8u * (gc & 1u);
+            const int rounds = (ve - vb + ngroups - 1) / ngroups;
+            for (int r = 0; r < rounds; ++r) {
+                const int v = vb + r * ngroups + grp;
+                const int lv = tab[rows[c] + r].z + lg;
+                cluster_vertex_srec<LANES, LAYOUT>(p, xs, xb, cs, cm, ys, pps, spans, bar, v, lv, v < ve, lane, lane_w,
+                                                   csize, blend, om);
+            }
+            const bool ok = mbar_wait(bar, (gc >> 1) & 1u, p.sw.status);
+            if (tid == 0 && ok && gc + 2 < total) mbar_expect(bar, walk_bytes(p, gc + 2));
+            alive = __syncthreads_and(ok) != 0;
+            if (!alive) break;
+        }
+        if (blend) cur ^= 1;
+    }
+    cluster_arrive();
+    cluster_wait();
+    if (!alive) return;
+    const float4* xf = sx + (cur ? n : 0);
+    for (int i = gt; i < p.nfree; i += nthreads) {
+        const float4 xi = xf[i];
+        p.xa[i] = xi;
+        if (p.finish) p.v[i] = damped_velocity(xi, p.xprev[i], p.v[i], p.h);
+    }
+}
+
 // ---- The adjoint sweeps of one sub-step as a cluster walk ----------------------------------------
 //
 // The same exchange for the adjoint's coloured Gauss-Seidel on (M/h^2 + H) lam = G: every CTA holds

@@ -979,6 +979,9 @@ struct PersistParams {
     int init_from_inertia;    // start from x = y
     int expected_blocks;      // arrivals the barrier waits for (gridDim.x in normal use)
     float h, hgx, hgy, hgz;
+    // the cluster walk with resident element data: per CTA at most srec_records records and
+    // srec_owned vertices, srec_slices (colour, round) slices
+    int srec_records, srec_owned, srec_slices;
 };
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {

@@ -106,8 +106,9 @@ static SweepFn pick_sweep(int lanes, int layout, int prefetch, bool cache) {
     }
 }
 
-// The cluster walk reads the factored records (layouts 3 and 4).
-template <int L> static void (*pick_cluster(int layout))(PersistParams) {
+// The cluster walk reads the factored records (layouts 3 and 4), from L2 or resident in shared memory.
+template <int L> static void (*pick_cluster(int layout, bool resident))(PersistParams) {
+    if (resident) return layout == 3 ? &k_cluster_walk_srec<L, 3> : &k_cluster_walk_srec<L, 4>;
     return layout == 3 ? &k_cluster_walk<L, 3> : &k_cluster_walk<L, 4>;
 }
 
@@ -162,6 +163,7 @@ struct vbd_solver {
     long long ninc = 0;
     bool ready = false, have_materials = false;
     std::vector<int> cstart;  // colour c = internal ids [cstart[c], cstart[c+1])
+    std::vector<int32_t> h_inc_off;  // incidence offsets of the internal vertices (host copy)
     vbd::DBuf<float4> x0, x1, pp, y, v, xprev;
     vbd::DBuf<int> perm, inc_off, inc_tet;
     vbd::DBuf<vbd::TetRec> rec, irec;
@@ -220,6 +222,12 @@ struct vbd_solver {
     // cluster holding the positions in shared memory (meshes of up to about 7,000 vertices)
     int persistent = 0;
     int cluster_ctas_opt = 0;                       // CTAs of the cluster walk (0 = from the colour sizes)
+    int cluster_resident = 1;  // the walk keeps each CTA's element records in shared memory where they fit
+    // the resident walk's plan for the mesh, kernel and CTA count it was made for
+    int sr_gen = -1, sr_ctas = 0, sr_records = 0, sr_owned = 0, sr_slices = 0;
+    const void* sr_fn = nullptr;
+    unsigned long long sr_smem = 0;
+    bool sr_ok = false;
     // launch shape resolved for the mesh, the kernel and the requested CTAs (the kernel's shared-memory
     // and cluster-size attributes are set per kernel)
     int cl_ctas = 0, cl_block = 0, cl_gen = -1, cl_req = 0;
@@ -734,7 +742,35 @@ struct vbd_solver {
         return check_launch();
     }
 
-    // A sub-step (predict and finish) or a solve as one cluster launch (vbd::k_cluster_walk).
+    // Per-CTA sizes of the resident walk for L lanes and `ctas` CTAs of kClusterMaxBlock threads: the
+    // (colour, round) slices, and the most records and vertices any CTA sweeps (the kernel derives
+    // the same plan, k_cluster_walk_srec).
+    void srec_plan(int L, int ctas, int* records, int* owned, int* slices) const {
+        const int gpc = vbd::kClusterMaxBlock / L, G = ctas * gpc;
+        int S = 0, rec_max = 0, own_max = 0;
+        for (int c = 0; c < C; ++c) S += (cstart[c + 1] - cstart[c] + G - 1) / G;
+        for (int k = 0; k < ctas; ++k) {
+            long long rec = 0, own = 0;
+            for (int c = 0; c < C; ++c) {
+                const int vb = cstart[c], ve = cstart[c + 1];
+                for (int r = 0; r * G < ve - vb; ++r) {
+                    const int vf = vb + r * G + k * gpc;
+                    const int cnt = std::max(0, std::min(vf + gpc, ve) - vf);
+                    own += cnt;
+                    if (cnt) rec += h_inc_off[vf + cnt] - h_inc_off[vf];
+                }
+            }
+            rec_max = (int)std::max<long long>(rec_max, rec);
+            own_max = (int)std::max<long long>(own_max, own);
+        }
+        *records = rec_max;
+        *owned = own_max;
+        *slices = S;
+    }
+
+    // A sub-step (predict and finish) or a solve as one cluster launch: vbd::k_cluster_walk_srec where
+    // the CTAs' element data fits in shared memory (and VBD_OPT_CLUSTER_RESIDENT allows it), else
+    // vbd::k_cluster_walk.
     int launch_cluster(int iters, float dtsr, bool accel, float rho, bool predict, bool finish, bool from_inertia,
                        float h, const float* hg) {
         const char* why = nullptr;
@@ -742,18 +778,58 @@ struct vbd_solver {
         VBD_TRY(upload_schedule(iters, accel, rho));
         const int L = lanes < 4 ? 4 : lanes;
         void (*fn)(vbd::PersistParams) = nullptr;
+        void (*fn_res)(vbd::PersistParams) = nullptr;
         switch (L) {
-            case 4: fn = vbd::pick_cluster<4>(layout); break;
-            case 8: fn = vbd::pick_cluster<8>(layout); break;
-            case 16: fn = vbd::pick_cluster<16>(layout); break;
-            default: fn = vbd::pick_cluster<32>(layout); break;
+            case 4: fn = vbd::pick_cluster<4>(layout, false); fn_res = vbd::pick_cluster<4>(layout, true); break;
+            case 8: fn = vbd::pick_cluster<8>(layout, false); fn_res = vbd::pick_cluster<8>(layout, true); break;
+            case 16: fn = vbd::pick_cluster<16>(layout, false); fn_res = vbd::pick_cluster<16>(layout, true); break;
+            default: fn = vbd::pick_cluster<32>(layout, false); fn_res = vbd::pick_cluster<32>(layout, true); break;
         }
         VBD_TRY(resolve_cluster(fn, L));
-        const vbd::PersistParams w = walk_params(iters, dtsr, accel, predict, finish, from_inertia, h, hg);
+        vbd::PersistParams w = walk_params(iters, dtsr, accel, predict, finish, from_inertia, h, hg);
+        size_t smem = cluster_smem();
+        if (cluster_resident) {
+            const void* f = reinterpret_cast<const void*>(fn_res);
+            if (!(sr_gen == shape_gen && sr_fn == f && sr_ctas == cl_ctas)) {
+                sr_gen = shape_gen;
+                sr_fn = f;
+                sr_ctas = cl_ctas;
+                sr_ok = false;
+                srec_plan(L, cl_ctas, &sr_records, &sr_owned, &sr_slices);
+                sr_smem = vbd::srec_layout(N, sr_records, sr_owned, sr_slices, C, layout).total;
+                int optin = 0;
+                CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+                if (sr_smem + 64 <= (unsigned long long)optin) {
+                    CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sr_smem));
+                    CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+                    cudaLaunchConfig_t q = {};
+                    q.gridDim = dim3(cl_ctas);
+                    q.blockDim = dim3(cl_block);
+                    q.dynamicSmemBytes = (size_t)sr_smem;
+                    cudaLaunchAttribute qa[1];
+                    qa[0].id = cudaLaunchAttributeClusterDimension;
+                    qa[0].val.clusterDim.x = cl_ctas;
+                    qa[0].val.clusterDim.y = 1;
+                    qa[0].val.clusterDim.z = 1;
+                    q.attrs = qa;
+                    q.numAttrs = 1;
+                    int clusters = 0;
+                    sr_ok = cudaOccupancyMaxActiveClusters(&clusters, fn_res, &q) == cudaSuccess && clusters >= 1;
+                    (void)cudaGetLastError();
+                }
+            }
+            if (sr_ok) {
+                fn = fn_res;
+                smem = (size_t)sr_smem;
+                w.srec_records = sr_records;
+                w.srec_owned = sr_owned;
+                w.srec_slices = sr_slices;
+            }
+        }
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(cl_ctas);
         cfg.blockDim = dim3(cl_block);
-        cfg.dynamicSmemBytes = cluster_smem();
+        cfg.dynamicSmemBytes = smem;
         cfg.stream = stream;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1232,6 +1308,7 @@ int vbd_solver_init(vbd_solver* s, int32_t N, int32_t T, const float* positions,
     CUDA_TRY(cudaMemcpy(s->y.p, hy.data(), b4, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->perm.p, perm.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->inc_off.p, inc_off.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice));
+    s->h_inc_off = inc_off;  // the cluster walk's resident-record plan reads it on the host
     CUDA_TRY(cudaMemcpy(s->inc_tet.p, inc_tet.data(), sizeof(int) * inc_tet.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->inc_vertex.p, inc_vertex.data(), sizeof(int) * inc_vertex.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->rec.p, rec.data(), sizeof(vbd::TetRec) * rec.size(), cudaMemcpyHostToDevice));
@@ -1767,6 +1844,9 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value) {
             if (value < 0 || value > 16) VBD_FAIL(VBD_ERR_INVALID_ARG, "cluster CTAs must be 0 (automatic) to 16");
             s->cluster_ctas_opt = value;
             return VBD_OK;
+        case VBD_OPT_CLUSTER_RESIDENT:
+            s->cluster_resident = value ? 1 : 0;
+            return VBD_OK;
         case VBD_OPT_L2_PREFETCH:
             s->l2_prefetch = value ? 1 : 0;
             return VBD_OK;
@@ -1820,6 +1900,7 @@ int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value) {
         case VBD_OPT_PDL: *value = s->pdl; return VBD_OK;
         case VBD_OPT_BLOCK: *value = s->block; return VBD_OK;
         case VBD_OPT_PERSISTENT: *value = s->persistent; return VBD_OK;
+        case VBD_OPT_CLUSTER_RESIDENT: *value = s->cluster_resident; return VBD_OK;
         case VBD_OPT_CLUSTER_CTAS:
             *value = s->cluster_ctas_opt > 0 || !s->ready ? s->cluster_ctas_opt
                                                            : s->cluster_auto_ctas(s->lanes < 4 ? 4 : s->lanes);
