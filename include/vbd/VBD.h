@@ -4,7 +4,7 @@
 // numIterations Gauss-Seidel colour sweeps with the Chebyshev blend, velocity update x 0.999) but
 // execute through libvbd_b200: the TetMesh's positions and velocities are uploaded, one
 // vbd_solver_step runs on the device, and positions, velocities and the inertial target are read
-// back.  Colouring and Dm^-1 / V0 are computed by the library bit-exactly with the reference.
+// back (or, with the VBDParams::deviceResident extension, stay on the device until syncToHost).  Colouring and Dm^-1 / V0 are computed by the library bit-exactly with the reference.
 // energyHistory is filled as the reference fills it: computeTotalEnergy after iterations 0, 10,
 // 20, ... of every sub-step (VBD.cpp:93-95), evaluated on the device inside the step (FP64 sums)
 // and read back once per step; simulate() clears it first and evaluates the energy once more after
@@ -38,6 +38,12 @@ struct VBDParams {
     // extensions
     bool usePerTetMaterials = false;   // use TetMesh::tetMu / tetLambda instead of mu / lambda
     int device = 0;                    // CUDA device of the solver
+    // Keep the state on the GPU between steps: step() uploads the mesh's positions and velocities
+    // only at the first step and after markHostChanged(), and reads nothing back; syncToHost(mesh)
+    // brings positions, velocities and the inertial target back (simulate() does so before each
+    // callback).  mVertPrevPos is not maintained in this mode.  Default: the reference's behaviour,
+    // every step reads the state from and writes it back to the TetMesh.
+    bool deviceResident = false;
 };
 
 class VBDsolver {
@@ -74,16 +80,18 @@ class VBDsolver {
             precomputeTetData(mesh);
         }
         ensureDevice(mesh);
-        vbdCheck(vbd_solver_set_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_set_positions");
-        vbdCheck(vbd_solver_set_velocities(gpu_, mesh.mVelocity.data()), "vbd_solver_set_velocities");
-        mesh.savePreviousPosition();
+        if (!params.deviceResident || deviceStale_) {
+            vbdCheck(vbd_solver_set_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_set_positions");
+            vbdCheck(vbd_solver_set_velocities(gpu_, mesh.mVelocity.data()), "vbd_solver_set_velocities");
+            deviceStale_ = false;
+        }
+        if (!params.deviceResident) mesh.savePreviousPosition();
         const float g[3] = {params.gravity[0], params.gravity[1], params.gravity[2]};
         vbdCheck(vbd_solver_step(gpu_, params.dt, params.substeps, params.numIterations, g,
                                  params.useAcceleration ? 1 : 0, params.accelerationRho),
                  "vbd_solver_step");
-        vbdCheck(vbd_solver_get_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_get_positions");
-        vbdCheck(vbd_solver_get_velocities(gpu_, mesh.mVelocity.data()), "vbd_solver_get_velocities");
-        vbdCheck(vbd_solver_get_inertia(gpu_, mesh.mInertia.data()), "vbd_solver_get_inertia");
+        hostStale_ = true;
+        if (!params.deviceResident) syncToHost(mesh);
         // the energies the step evaluated after iterations 0, 10, 20, ... (VBD.cpp:93-95)
         int32_t n = 0;
         vbdCheck(vbd_solver_energy_history(gpu_, nullptr, 0, &n, 0), "vbd_solver_energy_history");
@@ -96,6 +104,7 @@ class VBDsolver {
         energyHistory.clear();
         for (int frame = 0; frame < numFrames; ++frame) {
             step(mesh);
+            syncToHost(mesh);  // the callback and the caller see the frame's state
             // the frame's energy (VBD.cpp:318-319), from the state the step left on the device
             const Real energy = deviceEnergy();
             VBD_LOG("Frame " << frame << " completed, Energy: " << energy);
@@ -105,12 +114,32 @@ class VBDsolver {
     }
 
     // Elastic log-J Neo-Hookean energy of the mesh's current positions (VBD.cpp:258-288), summed
-    // in FP64 on the device.
+    // in FP64 on the device.  With deviceResident the GPU's positions are the current ones unless
+    // the host copy was marked changed.
     Real computeTotalEnergy(const TetMesh& mesh) const {
         ensureDevice(mesh);
-        vbdCheck(vbd_solver_set_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_set_positions");
+        if (!params.deviceResident || deviceStale_) {
+            vbdCheck(vbd_solver_set_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_set_positions");
+            if (params.deviceResident) vbdCheck(vbd_solver_set_velocities(gpu_, mesh.mVelocity.data()),
+                                                "vbd_solver_set_velocities");
+            deviceStale_ = false;
+        }
         return deviceEnergy();
     }
+
+    // deviceResident: positions, velocities and the inertial target back into the mesh, if a step
+    // has run since the last sync.  (Without deviceResident every step already does this.)
+    void syncToHost(TetMesh& mesh) const {
+        if (!gpu_ || !hostStale_) return;
+        vbdCheck(vbd_solver_get_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_get_positions");
+        vbdCheck(vbd_solver_get_velocities(gpu_, mesh.mVelocity.data()), "vbd_solver_get_velocities");
+        vbdCheck(vbd_solver_get_inertia(gpu_, mesh.mInertia.data()), "vbd_solver_get_inertia");
+        hostStale_ = false;
+    }
+
+    // deviceResident: the caller changed the mesh's positions or velocities; the next step (or
+    // computeTotalEnergy) uploads them.
+    void markHostChanged() { deviceStale_ = true; }
 
     const std::vector<std::vector<IdType>>& getVertexColors() const { return vertexColors; }
     const std::vector<Matrix3r>& getTetDmInv() const { return tetDmInv; }
@@ -138,6 +167,7 @@ class VBDsolver {
             precomputeTetData(mesh);
         }
         ensureDevice(mesh);
+        syncToHost(mesh);  // deviceResident: the mesh first catches up with the device's state
         const Real dt = params.dt / params.substeps;
         const Real dtsr = (Real)(1.0 / (dt * dt));
         vbdCheck(vbd_solver_set_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_set_positions");
@@ -215,6 +245,7 @@ class VBDsolver {
         devTets_ = mesh.numTets;
         matKey_.clear();
         syncMaterials(mesh);
+        deviceStale_ = hostStale_ = false;  // the device now holds the mesh's state
     }
 
     // Materials as the reference uses them: params.mu / lambda for every tet (VBD.cpp:214-215), or
@@ -242,6 +273,8 @@ class VBDsolver {
 
     mutable vbd_solver* gpu_ = nullptr;
     mutable size_t devVerts_ = 0, devTets_ = 0;
+    mutable bool hostStale_ = false;   // the device holds a newer state than the mesh
+    mutable bool deviceStale_ = true;  // the mesh holds a newer state than the device
     mutable std::vector<float> matKey_;
 };
 

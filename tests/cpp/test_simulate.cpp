@@ -1,7 +1,7 @@
 // Drives VBDsolver::simulate (VBD.cpp:313-330) through the C++ drop-in surface (include/vbd/VBD.h)
 // with a per-frame callback, as a caller of the reference would, and writes what a caller sees:
 // the final state, what the callback observed, and energyHistory.
-// Usage: test_simulate <input.bin> <output.bin>
+// Usage: test_simulate <input.bin> <output.bin> [resident]   (resident: VBDParams::deviceResident)
 // input:  int32 N, T, iterations, frames, substeps, use_acceleration; float32 density, mu, lambda,
 //         dt, rho; rest[3N] f32, x0[3N] f32, v0[3N] f32, tets[4T] i32, fixed[N] u8
 // output: positions[3N], velocities[3N] (f32); int32 callbacks, int32 frames_in_order,
@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <fstream>
 #include <iostream>
+#include <string>
 #include <vector>
 
 #include "VBD.h"
@@ -67,6 +68,7 @@ int main(int argc, char** argv) {
     params.mu = prm[1];
     params.lambda = prm[2];
     params.density = prm[0];
+    params.deviceResident = argc > 3 && std::string(argv[3]) == "resident";
 
     VBDsolver solver;
     solver.setParams(params);

@@ -97,7 +97,7 @@ def _ref_cases():
     return mod.CASES
 
 
-def run_simulate(m, iters, frames, substeps, accel, dt, rho, tmp_path):
+def run_simulate(m, iters, frames, substeps, accel, dt, rho, tmp_path, resident=False):
     if not os.path.exists(SIM_BIN):
         subprocess.run(["make", "-C", CPP_DIR], check=True, capture_output=True)
     inp = tmp_path / "sim_in.bin"
@@ -109,7 +109,8 @@ def run_simulate(m, iters, frames, substeps, accel, dt, rho, tmp_path):
         m.tets.astype(np.int32).tofile(f)
         m.fixed.astype(np.uint8).tofile(f)
     out = tmp_path / "sim_out.bin"
-    r = subprocess.run([SIM_BIN, str(inp), str(out)], capture_output=True, text=True)
+    r = subprocess.run([SIM_BIN, str(inp), str(out)] + (["resident"] if resident else []), capture_output=True,
+                       text=True)
     assert r.returncode == 0, r.stderr
     raw = open(out, "rb").read()
     n3 = 3 * m.num_verts
@@ -141,3 +142,18 @@ def test_simulate_matches_reference_fixtures(gpu_device, case, tmp_path):
     assert err < 1e-5
     assert len(out["ehist"]) == len(eh) == frames * sub * ((iters + 9) // 10)
     np.testing.assert_allclose(out["ehist"], eh, rtol=1e-4, atol=1e-4 * np.abs(eh).max())
+
+
+@pytest.mark.parametrize("case", ["beam", "block_accel_off_sub2", "cube6_stiff"])
+def test_simulate_device_resident_equals_default(gpu_device, case, tmp_path):
+    """VBDParams::deviceResident keeps the state on the GPU between steps (simulate reads it back
+    for each callback, nothing is uploaded after the first step): the same positions, velocities and
+    energyHistory bit for bit as the reference-style round trip every step."""
+    make, dt, iters, accel, rho, sub = _ref_cases()[case]
+    m = make()
+    a = run_simulate(m, iters, 10, sub, accel, dt, rho, tmp_path)
+    b = run_simulate(m, iters, 10, sub, accel, dt, rho, tmp_path, resident=True)
+    assert b["callbacks"] == 10 and b["in_order"] and b["positions_match"]
+    np.testing.assert_array_equal(a["x"], b["x"])
+    np.testing.assert_array_equal(a["v"], b["v"])
+    np.testing.assert_array_equal(a["ehist"], b["ehist"])
