@@ -40,9 +40,10 @@ struct VBDParams {
     int device = 0;                    // CUDA device of the solver
     // Keep the state on the GPU between steps: step() uploads the mesh's positions and velocities
     // only at the first step and after markHostChanged(), and reads nothing back; syncToHost(mesh)
-    // brings positions, velocities and the inertial target back (simulate() does so before each
-    // callback).  mVertPrevPos is not maintained in this mode.  Default: the reference's behaviour,
-    // every step reads the state from and writes it back to the TetMesh.
+    // brings positions, velocities, the inertial target and the steps' energyHistory entries back
+    // (simulate() does so before each callback).  mVertPrevPos is not maintained in this mode.
+    // Default: the reference's behaviour, every step reads the state from and writes it back to the
+    // TetMesh.
     bool deviceResident = false;
 };
 
@@ -92,15 +93,10 @@ class VBDsolver {
                  "vbd_solver_step");
         hostStale_ = true;
         if (!params.deviceResident) syncToHost(mesh);
-        // the energies the step evaluated after iterations 0, 10, 20, ... (VBD.cpp:93-95)
-        int32_t n = 0;
-        vbdCheck(vbd_solver_energy_history(gpu_, nullptr, 0, &n, 0), "vbd_solver_energy_history");
-        std::vector<double> e((size_t)n);
-        vbdCheck(vbd_solver_energy_history(gpu_, e.data(), n, &n, 1), "vbd_solver_energy_history");
-        for (double v : e) energyHistory.push_back((Real)v);
     }
 
     void simulate(TetMesh& mesh, int numFrames, std::function<void(int, TetMesh&)> callback = nullptr) {
+        syncToHost(mesh);  // earlier resident steps' state and energies first
         energyHistory.clear();
         for (int frame = 0; frame < numFrames; ++frame) {
             step(mesh);
@@ -129,11 +125,18 @@ class VBDsolver {
 
     // deviceResident: positions, velocities and the inertial target back into the mesh, if a step
     // has run since the last sync.  (Without deviceResident every step already does this.)
-    void syncToHost(TetMesh& mesh) const {
+    // The energies the steps since the last sync evaluated after iterations 0, 10, 20, ...
+    // (VBD.cpp:93-95) are appended to energyHistory here too.
+    void syncToHost(TetMesh& mesh) {
         if (!gpu_ || !hostStale_) return;
         vbdCheck(vbd_solver_get_positions(gpu_, mesh.mVertPos.data()), "vbd_solver_get_positions");
         vbdCheck(vbd_solver_get_velocities(gpu_, mesh.mVelocity.data()), "vbd_solver_get_velocities");
         vbdCheck(vbd_solver_get_inertia(gpu_, mesh.mInertia.data()), "vbd_solver_get_inertia");
+        int32_t n = 0;
+        vbdCheck(vbd_solver_energy_history(gpu_, nullptr, 0, &n, 0), "vbd_solver_energy_history");
+        std::vector<double> e((size_t)n);
+        vbdCheck(vbd_solver_energy_history(gpu_, e.data(), n, &n, 1), "vbd_solver_energy_history");
+        for (double v : e) energyHistory.push_back((Real)v);
         hostStale_ = false;
     }
 
