@@ -103,4 +103,7 @@ def test_identification_recovers_hidden_materials(gpu_device):
     print(f"loss {hist[0]:.4e} -> {hist[-1]:.4e}; E rel err {relE}, nu abs err {dnu}, final losses {final}, {info}")
     assert hist[-1] < 1e-3 * hist[0]
     assert np.all(np.diff(hist) <= 0.0)  # every accepted step lowers the loss
-    assert relE.max() < 0.05
+    # measured on a B200: E relative errors 4e-7, 1e-7, 2e-6, 2.9e-3; nu absolute errors 7e-8, 1e-8,
+    # 3e-7, 2.5e-4 (the last mesh, the stiffest, stops at loss 2e-5)
+    assert np.median(relE) < 1e-4 and relE.max() < 0.02
+    assert np.median(dnu) < 1e-4 and dnu.max() < 5e-3
