@@ -15,6 +15,8 @@
 //   * solveVertex / computeTetContribution (per-vertex CPU helpers) are not provided.
 #pragma once
 
+#include <algorithm>
+#include <cstddef>
 #include <functional>
 #include <vector>
 
@@ -253,20 +255,24 @@ class VBDsolver {
 
     // Materials as the reference uses them: params.mu / lambda for every tet (VBD.cpp:214-215), or
     // the mesh's per-tet values when usePerTetMaterials is set.
+    // The values last uploaded are kept in matKey_ (mu then lambda, per tet or uniform) and compared
+    // in place, so an unchanged per-tet material costs one read of the two arrays per step.
     void syncMaterials(const TetMesh& mesh) const {
-        std::vector<float> key;
         if (params.usePerTetMaterials) {
-            key = mesh.tetMu;
-            key.insert(key.end(), mesh.tetLambda.begin(), mesh.tetLambda.end());
-        } else {
-            key = {params.mu, params.lambda};
-        }
-        if (key == matKey_) return;
-        if (params.usePerTetMaterials)
+            const size_t T = mesh.tetMu.size();
+            if (matPerTet_ && matKey_.size() == 2 * T && mesh.tetLambda.size() == T &&
+                std::equal(mesh.tetMu.begin(), mesh.tetMu.end(), matKey_.begin()) &&
+                std::equal(mesh.tetLambda.begin(), mesh.tetLambda.end(), matKey_.begin() + (std::ptrdiff_t)T))
+                return;
             vbdCheck(vbd_solver_set_materials(gpu_, mesh.tetMu.data(), mesh.tetLambda.data()), "vbd_solver_set_materials");
-        else
+            matKey_.assign(mesh.tetMu.begin(), mesh.tetMu.end());
+            matKey_.insert(matKey_.end(), mesh.tetLambda.begin(), mesh.tetLambda.end());
+        } else {
+            if (!matPerTet_ && matKey_.size() == 2 && matKey_[0] == params.mu && matKey_[1] == params.lambda) return;
             vbdCheck(vbd_solver_set_uniform_material(gpu_, params.mu, params.lambda), "vbd_solver_set_uniform_material");
-        matKey_ = key;
+            matKey_ = {params.mu, params.lambda};
+        }
+        matPerTet_ = params.usePerTetMaterials;
     }
 
     void release() {
@@ -279,6 +285,7 @@ class VBDsolver {
     mutable bool hostStale_ = false;   // the device holds a newer state than the mesh
     mutable bool deviceStale_ = true;  // the mesh holds a newer state than the device
     mutable std::vector<float> matKey_;
+    mutable bool matPerTet_ = false;  // matKey_ holds per-tet values
 };
 
 }  // namespace VBD

@@ -1,12 +1,15 @@
 // Exercises the C++ drop-in surface (include/vbd/*.h) the way the reference's callers do:
 //   flow 1: VBDsolver::step(mesh) (VBD.cpp:60-101), all on the GPU;
 //   flow 2: the reference driver's GPU loop (main.cpp:215-232): host forwardStep,
-//           VBD_GPU_Solver::updateInertiaFromCPU / solveVBD / copyPositionsToCPU, host updateVelocity.
+//           VBD_GPU_Solver::updateInertiaFromCPU / solveVBD / copyPositionsToCPU, host updateVelocity;
+//   flow 3: VBDsolver::step with VBDParams::usePerTetMaterials: tet t starts with
+//           mu (1 + t%5 / 8), lambda (1 + t%3 / 4), and after steps / 2 steps mu of every even tet is
+//           multiplied by 1.5 (the solver must pick the change up).
 // Usage: test_cpp_api <input.bin> <output.bin> <obj path>
 // input:  int32 N, T, iterations, steps; float32 density, mu, lambda, dt, rho; rest[3N] f32,
 //         tets[4T] i32, fixed[N] u8
 // output: flow-1 positions[3N], velocities[3N], flow-2 positions[3N] (f32), flow-1 energy (f32),
-//         number of surface triangles (int32), colour count (int32)
+//         number of surface triangles (int32), colour count (int32), flow-3 positions[3N] (f32)
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -90,6 +93,23 @@ int main(int argc, char** argv) {
         mesh2.updateVelocity(subDt);
     }
 
+    // flow 3
+    TetMesh mesh3;
+    mesh3.initialize(pos, pos, density, tets, mu, lambda, fixedList);
+    for (int t = 0; t < T; ++t) {
+        mesh3.tetMu[t] = mu * (1.0f + 0.125f * (float)(t % 5));
+        mesh3.tetLambda[t] = lambda * (1.0f + 0.25f * (float)(t % 3));
+    }
+    VBDParams p3 = params;
+    p3.usePerTetMaterials = true;
+    VBDsolver solver3;
+    solver3.setParams(p3);
+    for (int s = 0; s < steps; ++s) {
+        if (s == steps / 2)
+            for (int t = 0; t < T; t += 2) mesh3.tetMu[t] *= 1.5f;
+        solver3.step(mesh3);
+    }
+
     const bool objOk = mesh.exportToObj(argv[3]);
     const int32_t nsurf = (int32_t)mesh.extractSurfaceFaces().size();
     std::ofstream out(argv[2], std::ios::binary);
@@ -100,5 +120,6 @@ int main(int argc, char** argv) {
     wr(out, &nsurf, 1);
     const int32_t nc = ncol;
     wr(out, &nc, 1);
+    wr(out, mesh3.mVertPos.data(), 3 * (size_t)N);
     return objOk ? 0 : 1;
 }

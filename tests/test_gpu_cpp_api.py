@@ -1,6 +1,7 @@
 """The C++ drop-in surface on the GPU: tests/cpp/test_cpp_api runs the reference's two calling
 patterns (VBDsolver::step, and the main.cpp loop over VBD_GPU_Solver) through include/vbd/*.h and
 libvbd_b200; results are checked against the oracle."""
+import dataclasses
 import importlib.util
 import os
 import subprocess
@@ -37,10 +38,28 @@ def run_cpp(m, iters, steps, dt, rho, tmp_path):
     assert r.returncode == 0, r.stderr
     raw = open(out, "rb").read()
     n3 = 3 * m.num_verts
-    f = np.frombuffer(raw[: 4 * (3 * n3 + 1)], np.float32)
-    tail = np.frombuffer(raw[4 * (3 * n3 + 1):], np.int32)
+    k = 4 * (3 * n3 + 1)
+    f = np.frombuffer(raw[:k], np.float32)
+    tail = np.frombuffer(raw[k:k + 8], np.int32)
+    x3 = np.frombuffer(raw[k + 8:], np.float32)
+    assert x3.size == n3
     return dict(x1=f[:n3].reshape(-1, 3), v1=f[n3:2 * n3].reshape(-1, 3), x2=f[2 * n3:3 * n3].reshape(-1, 3),
-                energy=float(f[3 * n3]), nsurf=int(tail[0]), ncol=int(tail[1]), obj=obj)
+                energy=float(f[3 * n3]), nsurf=int(tail[0]), ncol=int(tail[1]), obj=obj, x3=x3.reshape(-1, 3))
+
+
+def per_tet_flow_oracle(m, iters, steps, dt, rho):
+    """test_cpp_api's flow 3 by the FP32 oracle: VBDsolver::step with per-tet materials mu (1 + t%5 / 8),
+    lambda (1 + t%3 / 4), and mu of every even tet times 1.5 from step steps // 2 on."""
+    t = np.arange(m.num_tets)
+    mu = np.float32(m.mu[0]) * (np.float32(1.0) + np.float32(0.125) * (t % 5).astype(np.float32))
+    lam = np.float32(m.lam[0]) * (np.float32(1.0) + np.float32(0.25) * (t % 3).astype(np.float32))
+    mu2 = mu.copy()
+    mu2[::2] *= np.float32(1.5)
+    half = steps // 2
+    a = po.simulate(dataclasses.replace(m, mu=mu, lam=lam), half, dt, iters, (0.0, -9.8, 0.0), True, rho, precision=32)
+    b = po.simulate(dataclasses.replace(m, mu=mu2, lam=lam), steps - half, dt, iters, (0.0, -9.8, 0.0), True, rho,
+                    precision=32, x0=a["x"], v0=a["v"])
+    return b["x"]
 
 
 def wrapper_flow_oracle(m, iters, steps, dt, rho):
@@ -73,6 +92,10 @@ def test_cpp_surface_matches_oracle(gpu_device, tmp_path):
     assert np.abs(out["v1"] - o["v"]).max() < 1e-3 * np.abs(o["v"]).max()
     w = wrapper_flow_oracle(m, s["iterations"], 10, s["dt"], s["rho"])
     assert rel_err(out["x2"], w, m) < 1e-5
+    # per-tet materials through VBDParams::usePerTetMaterials, changed half way
+    p = per_tet_flow_oracle(m, s["iterations"], 10, s["dt"], s["rho"])
+    assert rel_err(out["x3"], p, m) < 1e-5
+    assert rel_err(out["x3"], o["x"], m) > 1e-4  # the materials made a difference
     assert out["ncol"] == 8
     assert out["nsurf"] == 2 * 2 * (16 * 4 + 16 * 4 + 4 * 4)
     lines = open(out["obj"]).read().splitlines()
