@@ -41,10 +41,12 @@ typedef enum vbd_status {
 
 typedef struct vbd_solver vbd_solver; /* opaque; owns all device memory of one mesh (or batch) */
 
-/* Library version, as 10000*major + 100*minor + patch. */
+/* Library version, as 10000*major + 100*minor + patch (no reference counterpart). */
 int vbd_version(void);
 
-/* Message of the last failing call on this thread ("" if none). */
+/* Message of the last failing call on this thread ("" if none).  No reference counterpart: the
+ * reference's calls return void and leave CUDA errors unchecked; every call here returns a
+ * vbd_status. */
 const char* vbd_last_error(void);
 
 /* ------------------------------------------------------------------------------------------
@@ -112,7 +114,8 @@ int vbd_pin_low_fraction(int32_t num_verts, const float* positions, int32_t axis
  * step loop of VBD::VBDsolver (VBD.cpp:60-112).
  * ------------------------------------------------------------------------------------------ */
 
-/* Creates a handle on CUDA device `device`.  `cuda_stream` is a cudaStream_t (may be null: the
+/* Replaces the VBD_GPU_Solver constructor (VBD_GPU_Wrapper.h:9-11).
+ * Creates a handle on CUDA device `device`.  `cuda_stream` is a cudaStream_t (may be null: the
  * handle then creates its own non-blocking stream).  Fails with VBD_ERR_NO_DEVICE if the device
  * is absent or is not compute capability 10.0. */
 int vbd_solver_create(vbd_solver** out, int device, void* cuda_stream);
@@ -219,10 +222,11 @@ int vbd_solver_backward(vbd_solver* s, const float* dl_dx, const float* dl_dv, i
                         float adjoint_rho, float* dl_dx0, float* dl_dv0, float* dl_dmu, float* dl_dlambda);
 
 /* Waits for all work queued on the handle's stream and reports sticky device errors, and
- * VBD_ERR_TIMEOUT if a grid barrier of the persistent kernel gave up since the last sync. */
+ * VBD_ERR_TIMEOUT if a grid barrier of the persistent kernel gave up since the last sync.  No
+ * reference counterpart: the reference's calls are synchronous. */
 int vbd_solver_sync(vbd_solver* s);
 
-/* Failure-detection self-test: launches the persistent kernel with one barrier arrival missing and
+/* Failure-detection self-test (no reference counterpart): launches the persistent kernel with one barrier arrival missing and
  * a poll limit of spin_limit, so its first grid barrier can never complete.  Every block gives up
  * after spin_limit polls and exits; *timed_out receives 1 if the device recorded the timeout. */
 int vbd_solver_barrier_selftest(vbd_solver* s, int64_t spin_limit, int32_t* timed_out);
@@ -357,17 +361,18 @@ int vbd_solver_set_option(vbd_solver* s, int32_t option, int32_t value);
 int vbd_solver_get_option(vbd_solver* s, int32_t option, int32_t* value);
 
 /* Per-colour launch shape (no reference counterpart; the reference's kernel runs 16 threads per
- * vertex for every colour, VBD_GPU_Wrapper.cu:349): colour c of the sweep runs lanes[c] threads per
- * vertex (1, 2, 4, 8, 16 or 32), and its record prefetch follows the lane count as VBD_OPT_PREFETCH
- * describes.  lanes = NULL goes back to VBD_OPT_LANES for every colour.  Same results as the
+ * vertex for every colour, VBD_GPU_Wrapper.cu:320-321): colour c of the sweep runs lanes[c]
+ * threads per vertex (1, 2, 4, 8, 16 or 32), and its record prefetch follows the lane count as
+ * VBD_OPT_PREFETCH describes.  lanes = NULL goes back to VBD_OPT_LANES for every colour.  Same results as the
  * uniform shape up to the order of the per-vertex sums.  A new mesh (vbd_solver_init) clears it.
  * get_colour_lanes writes the lane count each colour runs. */
 int vbd_solver_set_colour_lanes(vbd_solver* s, int32_t num_colours, const int32_t* lanes);
 int vbd_solver_get_colour_lanes(vbd_solver* s, int32_t num_colours, int32_t* lanes);
 
-/* Autotuner: times `repeats` steps of `iterations` sweeps (dt, no gravity, Chebyshev 0.9) for each
- * launch configuration it tries and keeps the fastest, then restores the simulation state
- * (positions, velocities, inertia, counters) it started from.  In order:
+/* Autotuner (no reference counterpart: the reference launches one 16-thread block per vertex,
+ * VBD_GPU_Wrapper.cu:320-321): times `repeats` steps of `iterations` sweeps (dt, no gravity,
+ * Chebyshev 0.9) for each launch configuration it tries and keeps the fastest, then restores the
+ * simulation state (positions, velocities, inertia, counters) it started from.  In order:
  *   1. uniform launch shapes from a fixed list -- threads per vertex, record layout, prefetch,
  *      programmatic dependent launch, block size;
  *   2. the factored records' L2 policy (VBD_OPT_RECORD_CACHE with VBD_OPT_RECORD_PERSIST_MB 0, 32
@@ -406,13 +411,14 @@ int vbd_ip_energy_noalloc(int32_t num_verts, int32_t num_tets, const float* posi
                           const float* vertex_mass, const int32_t* tets, const float* dm_inv, const float* rest_vol,
                           const float* tet_mu, const float* tet_lambda, float h, double* out, void* cuda_stream);
 
-/* Sizes of the uploaded mesh: vertices, tets, colours. */
+/* Sizes of the uploaded mesh: vertices, tets, colours (no reference counterpart). */
 int vbd_solver_info(vbd_solver* s, int32_t* num_verts, int32_t* num_tets, int32_t* num_colours);
 
-/* Number of kernels this handle launched since creation (graph replays count their nodes). */
+/* Number of kernels this handle launched since creation (graph replays count their nodes; no
+ * reference counterpart). */
 int vbd_solver_kernel_launches(vbd_solver* s, int64_t* launches);
 
-/* With VBD_OPT_KERNEL_TIMING on: summed device time (ms) of the colour-sweep kernels timed since
+/* With VBD_OPT_KERNEL_TIMING on (no reference counterpart): summed device time (ms) of the colour-sweep kernels timed since
  * the last reset, their count, and the algorithmic bytes they moved (per free vertex swept:
  * 60 B per incident tet -- tet id, 4 vertex ids, Dm^-1, V0 -- plus 96 B of vertex state).
  * Completes the timed work first. */
