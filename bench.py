@@ -659,7 +659,7 @@ def bench_material_id(local, stream, autotune=True):
     """Batched material identification: 64 beams (Lx U{8..40}, Ly = Lz U{3..8}), hidden (E, nu) as the
     batched configuration, targets from a 20-step forward under gravity; per-mesh gradients of
     (log E, nu) from one batched forward + adjoint vs central finite differences of the batched
-    forward (step 1e-2) at the initial guess, then 50 per-mesh trust-region quasi-Newton iterations from E = 1e5,
+    forward (step 1e-2) at the initial guess, then 50 per-mesh trust-region iterations from E = 1e5,
     nu = 0.3."""
     import torch
 
@@ -701,11 +701,12 @@ def bench_material_id(local, stream, autotune=True):
                    "2.2e-3 at 3e-3, 8.5e-4 at 1e-2, whether the adjoint runs 50 or 1,000 sweeps and the forward "
                    "100 or 1,000 iterations; checked against FP64 finite differences at converged iterations in "
                    "tests/test_gpu_material_id.py",
-        "optimizer": "per-mesh trust-region quasi-Newton (2x2 BFGS on log E, nu/0.1) with E kept in [5e3, 2e6] "
-                     "(the configuration draws it from [1e4, 1e6]); every iteration is one batched forward + adjoint "
-                     "of all meshes; a mesh whose trials fail twice in a row, or whose last 5 accepted steps together "
-                     "lowered its loss by less than 10% (the forward far from converged, so the implicit gradient "
-                     "misleads), takes central finite differences of the batched forward from then on",
+        "optimizer": "per-mesh trust-region descent on (log E, nu/0.1) with E kept in [5e3, 2e6] (the configuration "
+                     "draws it from [1e4, 1e6]); every iteration is one batched forward + adjoint of all meshes; a mesh "
+                     "steps by a 2x2 BFGS estimate from the adjoint's gradients until its trials fail twice in a row, or "
+                     "its last 5 accepted steps together lowered its loss by less than 10% (the forward far from "
+                     "converged, so the implicit gradient misleads); from then on it takes Levenberg-Marquardt steps "
+                     "from the central-difference Jacobian of its final positions (four batched forwards)",
         "meshes_on_finite_differences": id_info["fd_meshes"],
         "batched_forward_adjoints": id_info["forward_backwards"],
         "batched_forwards": id_info["forwards"],

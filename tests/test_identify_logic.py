@@ -24,7 +24,8 @@ class FakeProblem:
 
     def forward(self, logE, nu, record=False):
         self.forwards += 1
-        return np.stack([np.asarray(logE, np.float64), np.asarray(nu, np.float64) / mid.NU_SCALE], axis=1)
+        self.last_x = np.stack([np.asarray(logE, np.float64), np.asarray(nu, np.float64) / mid.NU_SCALE], axis=1)
+        return self.last_x
 
     def losses(self, x, targets):
         return np.sum((x - targets) ** 2, axis=1)

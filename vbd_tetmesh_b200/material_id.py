@@ -4,7 +4,8 @@ Every mesh of the batch advances in one solver (colour c of all meshes in one la
 recorded forward and one backward pass (vbd_solver_record / vbd_solver_backward) give the
 per-tet gradients dL/dmu, dL/dlambda of the loss L = sum_m sum_i |x_i - x*_i|^2, which chain to
 each mesh's (log E, nu) through mu = E / (2 (1 + nu)), lambda = E nu / ((1 + nu)(1 - 2 nu)).
-Each mesh's (log E, nu) moves by its own trust-region quasi-Newton step (identify); one trial of all
+Each mesh's (log E, nu) moves by its own trust-region step (identify: quasi-Newton on the
+adjoint's gradients, or Levenberg-Marquardt on a finite-difference Jacobian); one trial of all
 meshes costs one batched forward + adjoint.  Finite-difference checks need only two
 batched forwards per parameter, since the meshes are independent.
 """
@@ -63,6 +64,7 @@ class Problem:
     solver: object
     tet_mesh: np.ndarray
     settings: Settings = field(default_factory=Settings)
+    last_x: np.ndarray | None = None
 
     @classmethod
     def create(cls, meshes, settings=None, device=0, stream=None):
@@ -78,7 +80,8 @@ class Problem:
         return mu, lam, dmu, dlam
 
     def forward(self, logE, nu, record=False):
-        """Final positions after `steps` steps from rest with per-mesh (log E, nu)."""
+        """Final positions after `steps` steps from rest with per-mesh (log E, nu); also kept in
+        self.last_x (loss_and_grad runs one forward)."""
         st = self.settings
         mu, lam, _, _ = self._materials(logE, nu)
         s = self.solver
@@ -88,7 +91,8 @@ class Problem:
         s.record(st.checkpoint if record else 0)
         for _ in range(st.steps):
             s.step(st.dt, st.iterations, st.gravity, True, st.rho)
-        return s.get_positions().astype(np.float64)
+        self.last_x = s.get_positions().astype(np.float64)
+        return self.last_x
 
     def losses(self, x, targets):
         """Per-mesh loss sum_i |x_i - x*_i|^2."""
@@ -130,27 +134,40 @@ NU_SCALE = 0.1  # nu is optimised as nu / NU_SCALE, so both coordinates move on 
 
 def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), E_bounds=(5e3, 2e6), radius0=(1.0, 0.5),
              armijo=1e-4, fd_after=2, fd_step=1e-3, converged=1e-7, stall_window=5, stall_gain=0.1, trace=None):
-    """Per-mesh trust-region quasi-Newton descent on z = (log E, nu / NU_SCALE).
+    """Per-mesh trust-region descent on z = (log E, nu / NU_SCALE).
 
-    Every mesh keeps its own 2x2 BFGS inverse-Hessian estimate and its own trust radius (per
-    coordinate, initially radius0).  Each outer iteration evaluates every mesh's trial point in one
-    batched forward + adjoint; a mesh whose loss falls by the Armijo condition accepts the trial and
-    widens its radius, the others halve it.  The adjoint differentiates each step as converged; on
-    stiff, nearly incompressible meshes the forward's fixed iteration count leaves the step far
-    from converged, so that gradient can point away from descent.  A mesh whose trial has been
-    rejected fd_after times in a row, while its loss is still above `converged` times its initial
-    loss (below that, rejections come from FP32 noise in the loss), therefore takes central finite
-    differences of the batched forward (step fd_step) as its gradient from then on; those forwards
-    are run only while some mesh needs them.  The same switch happens when a mesh's last
-    stall_window accepted steps together lowered its loss by less than stall_gain of it: steps that
-    are accepted but barely help also mark a gradient that does not point downhill.  nu is kept
-    inside nu_bounds and E inside E_bounds (the batched configuration draws E from [1e4, 1e6];
-    beyond it a very stiff beam barely moves, and the flat loss there holds a descent back).
+    Every mesh keeps its own trust radius (per coordinate, initially radius0).  Each outer
+    iteration evaluates every mesh's trial point in one batched forward + adjoint; a mesh whose loss
+    falls by the Armijo condition accepts the trial and widens its radius, the others halve it.
+    Steps come from one of two models per mesh:
+    * the adjoint's gradient with a 2x2 BFGS inverse-Hessian estimate;
+    * once a mesh is on finite differences, a Levenberg-Marquardt step from the Jacobian J of its
+      final positions with respect to z, taken by central differences (step fd_step) of the batched
+      forward: (J^T J + m diag(J^T J)) d = -J^T r with r the positions minus the targets, the loss's
+      gradient being 2 J^T r; m falls by 3 after an accepted step and grows by 4 after a rejected
+      one.  The loss is a sum of squared residuals, so J^T J is its Gauss-Newton Hessian, which
+      follows a long, curved (log E, nu) valley where a quasi-Newton estimate from two gradients
+      crawls.  The four forwards of J are the ones the finite-difference gradient needs anyway; they
+      run only while some mesh needs them, all meshes in each.
+    The adjoint differentiates each step as converged; on stiff, nearly incompressible meshes the
+    forward's fixed iteration count leaves the step far from converged, so that gradient can point
+    away from descent.  A mesh whose trial has been rejected fd_after times in a row, while its loss
+    is still above `converged` times its initial loss (below that, rejections come from FP32 noise
+    in the loss), therefore switches to finite differences for good.  The same switch happens when a
+    mesh's last stall_window accepted steps together lowered its loss by less than stall_gain of it:
+    steps that are accepted but barely help also mark a gradient that does not point downhill.  nu
+    is kept inside nu_bounds and E inside E_bounds (the batched configuration draws E from [1e4,
+    1e6]; beyond it a very stiff beam barely moves, and the flat loss there holds a descent back).
+
+    `problem` provides forward(logE, nu) -> final positions (N, 3), which it also leaves in
+    problem.last_x, losses(x, targets) -> per-mesh losses, loss_and_grad(logE, nu, targets) (one
+    forward, then the adjoint) and batch.vert_offsets.
 
     Returns (logE, nu, history of the total loss at the accepted points, per-mesh final losses, info)
     with info = dict(fd_meshes, forwards, forward_backwards).  A list passed as `trace` receives,
     per outer iteration, a dict of per-mesh arrays: z, loss, trial loss, accepted, radius, use_fd."""
     M = len(problem.batch.meshes)
+    offs = np.asarray(problem.batch.vert_offsets)
     z = np.stack([np.asarray(logE0, np.float64), np.asarray(nu0, np.float64) / NU_SCALE], axis=1)
     lo = np.array([np.log(E_bounds[0]), nu_bounds[0] / NU_SCALE])
     hi = np.array([np.log(E_bounds[1]), nu_bounds[1] / NU_SCALE])
@@ -160,30 +177,42 @@ def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), E_b
     def evaluate(zz):
         counts["forward_backwards"] += 1
         L, gE, gN = problem.loss_and_grad(zz[:, 0], zz[:, 1] * NU_SCALE, targets)
-        return L, np.stack([gE, gN * NU_SCALE], axis=1)
+        return L, np.stack([gE, gN * NU_SCALE], axis=1), np.array(problem.last_x, np.float64, copy=True)
 
-    def fd_gradient(zz):
-        g = np.zeros_like(zz)
+    def per_mesh(a):
+        """Sums of a per-vertex quantity over each mesh's vertices."""
+        return np.add.reduceat(a, offs[:-1])
+
+    def gauss_newton(zz, xx):
+        """J^T J (M, 2, 2) and J^T r (M, 2) of every mesh at zz, whose positions are xx, from central
+        differences of the batched forward (four forwards)."""
+        J = []
         for c, h in ((0, fd_step), (1, fd_step / NU_SCALE)):
-            Ls = []
+            xs = []
             for sign in (1.0, -1.0):
                 zt = zz.copy()
                 zt[:, c] += sign * h
                 counts["forwards"] += 1
-                Ls.append(problem.losses(problem.forward(zt[:, 0], zt[:, 1] * NU_SCALE), targets))
-            g[:, c] = (Ls[0] - Ls[1]) / (2.0 * h)
-        return g
+                xs.append(np.asarray(problem.forward(zt[:, 0], zt[:, 1] * NU_SCALE), np.float64))
+            J.append((xs[0] - xs[1]) / (2.0 * h))
+        r = xx - targets
+        A = np.empty((M, 2, 2))
+        b = np.empty((M, 2))
+        for i in range(2):
+            b[:, i] = per_mesh(np.sum(J[i] * r, axis=1))
+            for k in range(i, 2):
+                A[:, i, k] = A[:, k, i] = per_mesh(np.sum(J[i] * J[k], axis=1))
+        return A, b
 
-    L, g = evaluate(z)
+    L, g, X = evaluate(z)
     L0 = L.copy()
     hist = [float(L.sum())]
     radius = np.tile(np.asarray(radius0, np.float64), (M, 1))
     Hinv = np.zeros((M, 2, 2))
     rejects = np.zeros(M, int)
     use_fd = np.zeros(M, bool)
+    damping = np.full(M, 1e-3)  # Levenberg-Marquardt parameter of the finite-difference meshes
     accepted_losses = [[float(L[m])] for m in range(M)]  # loss after each accepted step
-    zp, gp = z.copy(), g.copy()          # a finite-difference mesh's previous point and gradient
-    have_prev = np.zeros(M, bool)
 
     def reset(m):
         Hinv[m] = np.eye(2) * (radius[m].min() / max(np.abs(g[m]).max(), 1e-300))
@@ -198,40 +227,43 @@ def identify(problem, targets, logE0, nu0, outer=50, nu_bounds=(0.05, 0.48), E_b
     for m in range(M):
         reset(m)
     for _ in range(outer):
-        if use_fd.any():
-            gf = fd_gradient(z)
-            for m in np.flatnonzero(use_fd):
-                if not have_prev[m]:  # just switched: start the curvature estimate afresh
-                    g[m] = gf[m]
-                    reset(m)
-                elif np.any(z[m] != zp[m]):
-                    bfgs(m, z[m] - zp[m], gf[m] - gp[m])
-                zp[m], gp[m], have_prev[m] = z[m], gf[m], True
-            g[use_fd] = gf[use_fd]
         d = -np.einsum("mij,mj->mi", Hinv, g)
+        if use_fd.any():
+            A, b = gauss_newton(z, X)
+            for m in np.flatnonzero(use_fd):
+                g[m] = 2.0 * b[m]
+                Am = A[m] + damping[m] * np.diag(np.diag(A[m])) + 1e-300 * np.eye(2)
+                try:
+                    d[m] = -np.linalg.solve(Am, b[m])
+                except np.linalg.LinAlgError:
+                    d[m] = -b[m] * radius[m].min() / max(np.abs(b[m]).max(), 1e-300)
         for m in range(M):
             if g[m] @ d[m] >= 0.0:  # not a descent direction: restart from a scaled gradient step
                 reset(m)
                 d[m] = -Hinv[m] @ g[m]
         d *= np.minimum(1.0, np.min(radius / np.maximum(np.abs(d), 1e-300), axis=1))[:, None]
         trial = np.clip(z + d, lo, hi)
-        Lt, gt = evaluate(trial)
+        Lt, gt, Xt = evaluate(trial)
         step = trial - z
         ok = Lt <= L + armijo * np.einsum("mi,mi->m", g, step)
-        if use_fd.any():
-            gt[use_fd] = g[use_fd]  # refreshed by finite differences at the next iteration
         for m in range(M):
             if not ok[m]:
                 radius[m] *= 0.5
                 rejects[m] += 1
-                if rejects[m] >= fd_after and L[m] > converged * L0[m]:
+                if use_fd[m]:
+                    damping[m] *= 4.0
+                elif rejects[m] >= fd_after and L[m] > converged * L0[m]:
                     use_fd[m] = True
                 continue
             rejects[m] = 0
             radius[m] = np.minimum(2.0 * radius[m], 4.0 * np.asarray(radius0))
-            if not use_fd[m]:
+            if use_fd[m]:
+                damping[m] = max(damping[m] / 3.0, 1e-12)
+            else:
                 bfgs(m, trial[m] - z[m], gt[m] - g[m])
-            z[m], L[m], g[m] = trial[m], Lt[m], gt[m]
+                g[m] = gt[m]
+            z[m], L[m] = trial[m], Lt[m]
+            X[offs[m]:offs[m + 1]] = Xt[offs[m]:offs[m + 1]]
             hist_m = accepted_losses[m]
             hist_m.append(float(Lt[m]))
             if (not use_fd[m] and len(hist_m) > stall_window and L[m] > converged * L0[m]
