@@ -202,8 +202,18 @@ def meshgen_settings():
     return meshgen.CUBE_SETTINGS
 
 
+def nvsmi_device(local: int) -> str:
+    """nvidia-smi's name for CUDA device `local` of this process: the local-th entry of
+    CUDA_VISIBLE_DEVICES when that is set (an index or a UUID, both of which nvidia-smi --id
+    takes), else the index itself."""
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    ids = [v.strip() for v in vis.split(",") if v.strip()]
+    return ids[local] if local < len(ids) else str(local)
+
+
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples during the timed region."""
+    """nvidia-smi clock / throttle-reason samples during the timed region (device_index is the CUDA
+    device of this process; the sampler reads the same GPU under any CUDA_VISIBLE_DEVICES)."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -221,7 +231,8 @@ class ClockSampler:
             os.makedirs(out_dir, exist_ok=True)
             self.path = os.path.join(out_dir, f"clocks_rank{self.device_index}.csv")
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                ["nvidia-smi", f"--id={nvsmi_device(self.device_index)}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits",
                  "-lms", "20"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None

@@ -58,3 +58,14 @@ def test_clock_sampler_without_nvidia_smi(tmp_path, monkeypatch):
     c.wait_first_sample(timeout=0.2)
     c.mark()
     assert c.stop() is None
+
+
+def test_sampler_reads_the_gpu_behind_cuda_visible_devices(monkeypatch):
+    """CUDA device k of the process is the k-th entry of CUDA_VISIBLE_DEVICES, which is what
+    nvidia-smi --id must be given (an index or a UUID)."""
+    monkeypatch.delenv("CUDA_VISIBLE_DEVICES", raising=False)
+    assert bench.nvsmi_device(3) == "3"
+    monkeypatch.setenv("CUDA_VISIBLE_DEVICES", "5,2")
+    assert bench.nvsmi_device(0) == "5" and bench.nvsmi_device(1) == "2"
+    monkeypatch.setenv("CUDA_VISIBLE_DEVICES", "GPU-1234abcd")
+    assert bench.nvsmi_device(0) == "GPU-1234abcd"
